@@ -1,0 +1,354 @@
+"""Benchmark: atom-steps/s of energy + forces + stress on one or more B200s.
+
+A step is one evaluation (E, F, dE/dh for every structure) of the batched
+mixed-size workload: 4096 independent periodic ABX3 supercells with nx, ny,
+nz uniform in {1..4} (12-768 atoms, about 768k atoms), per-structure strain
+up to 5 % and N(0, 0.15 Bohr) jitter (seed 4 + rank), synthetic 5-element
+potential with 280 symmetry functions per element and 280-25-25-1 networks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...   # the CPU restatement on the host cores
+
+value = atoms x steps / (device time of the K steps, max over ranks), inputs
+resident in HBM (C ABI hdnnp_eval_batch_device); e2e = the same through
+hdnnp_eval_batch with pinned host buffers (H2D of Z/positions/cells and D2H of
+energies/forces/dE/dh inside every timed step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__  # noqa: E402
+
+POT_DIR = os.path.join(ROOT, "tests", "golden", "abx3")
+METRIC = "atom-steps/s (E+F+stress)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--structs", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=256, help="structures in the CPU baseline sample")
+    ap.add_argument("--lean", action="store_true",
+                    help="device-resident steps only (no e2e, peaks or CPU baseline): for profiler runs")
+    return ap.parse_args()
+
+
+def workload(W, n, seed):
+    structs = W.config_c4(n_struct=n, seed=seed)
+    off, Z, pos, lat, per = W.concat(structs)
+    latf = np.concatenate([l.ravel(order="F") for l in lat])
+    return structs, off, Z, pos, per, latf
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def start(self):
+        q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+            "clocks_event_reasons.sw_power_cap"
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                    if out.returncode == 0 and out.stdout.strip():
+                        self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._th = threading.Thread(target=run, daemon=True)
+        self._th.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 5 + k and s[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks(torch):
+    """FP64 and FP32 (no TF32) GEMM throughput of this GPU via cuBLAS (TFLOP/s),
+    the measured denominators for the symmetry-function kernels' CUDA-core
+    arithmetic; HBM and bf16 come from MEASURED_PEAKS.json."""
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for name, dt, n in (("fp64", torch.float64, 8192), ("fp32", torch.float32, 8192)):
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out[name] = 2 * n ** 3 / best / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    torch.cuda.empty_cache()
+    return out
+
+
+# FP64 operations per work unit of the symmetry-function kernels, counted
+# from the arithmetic in csrc/symfn.cu (additions, multiplications, FMAs as
+# 2; sqrt/exp/tanh/div each counted as one operation).
+FLOPS = {
+    "sf_values": {"entries": 25, "pairs": 39, "g4_terms": 10.5, "g2_terms": 6},
+    "sf_gradients": {"entries": 50, "pairs": 151, "g4_terms": 17.5, "g2_terms": 13},
+}
+
+
+def kernel_flops(stage, counters, evals):
+    per = FLOPS[stage]
+    return sum(per[k] * counters[k] for k in per) / max(evals, 1)
+
+
+def cpu_baseline(structs, sample, seed=0):
+    """The FP64 oracle (C++ restatement of the reference, OpenMP over atoms,
+    all host threads) on a seeded sample of the workload's structures."""
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    m = O.Model(POT_DIR)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(len(structs), size=min(sample, len(structs)), replace=False)
+    atoms = 0
+    t0 = time.perf_counter()
+    for k in idx:
+        s = structs[int(k)]
+        m.eval(s["Z"], s["pos"], s["lat"])
+        atoms += len(s["Z"])
+    dt = time.perf_counter() - t0
+    return {"value": atoms / dt, "unit": "atom-steps/s", "cores": O.max_threads(), "kind": "port",
+            "sample": f"{len(idx)} of the workload's structures ({atoms} atoms), one E+F+stress evaluation each, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's algorithm on the host cores.  The
+    Fortran reference cannot be built in this image (no Fortran compiler), so
+    its C++ restatement (the oracle, same loops, OpenMP over atoms) runs it."""
+    if rank != 0:
+        return
+    W = __graft_entry__.load_package().workloads
+    structs, off, *_ = workload(W, args.structs, 4)
+    steps = []
+    base = None
+    for it in range(args.warmup + args.steps):
+        b = cpu_baseline(structs, max(8, args.cpu_sample // 4), seed=it)
+        if it >= args.warmup:
+            steps.append(b["value"])
+        base = b
+    v = float(np.mean(steps))
+    line = {"metric": METRIC, "value": v, "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "batched mixed sizes: 4096 periodic ABX3 supercells (12-768 atoms), seed 4",
+                       "step": "E+F+stress of a seeded sample of the structures (atom-steps/s scale-free)"},
+            "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": base["cores"], "kind": "port",
+                             "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pkg = __graft_entry__.load_package()
+    from hdnnp_b200 import engine
+
+    W = pkg.workloads
+    structs, off, Z, pos, per, latf = workload(W, args.structs, 4 + rank)
+    natoms = int(off[-1])
+    nstruct = len(structs)
+    pot = engine.Hdnnp.from_runner(POT_DIR, device=local)
+    pot.set_precision(engine.HDNNP_PREC_MIXED if args.precision == "mixed" else engine.HDNNP_PREC_FP64)
+
+    # device-resident inputs / outputs (torch only as the allocator)
+    Zd = torch.from_numpy(Z).cuda()
+    posd = torch.from_numpy(pos).cuda()
+    Ed = torch.zeros(nstruct, dtype=torch.float64, device="cuda")
+    Fd = torch.zeros(natoms, 3, dtype=torch.float64, device="cuda")
+    Ld = torch.zeros(nstruct, 9, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream is NULL)
+    L = engine.lib()
+    import ctypes as C
+
+    def step_device():
+        code = L.hdnnp_eval_batch_device(
+            pot._c, nstruct, off.ctypes.data_as(C.POINTER(C.c_int64)), None, C.c_void_p(Zd.data_ptr()),
+            C.c_void_p(posd.data_ptr()), per.ctypes.data_as(C.POINTER(C.c_int32)),
+            latf.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(Ed.data_ptr()), C.c_void_p(Fd.data_ptr()),
+            C.c_void_p(Ld.data_ptr()), C.c_void_p(stream.cuda_stream))
+        engine._check(code)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- value: inputs resident in HBM
+    for _ in range(args.warmup):
+        step_device()
+    pot.profile(reset=True)
+    pot.set_profiling(True)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_device()
+        e1.record(stream)
+        times.append((e0, e1))
+    barrier()
+    clk = clocks.stop()
+    pot.set_profiling(False)
+    stage_ms, counters = pot.profile(reset=True)
+    dev_s = sum(a.elapsed_time(b) for a, b in times) / 1e3
+    launches_per_step = pot.launches()
+    t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_s = float(t.item())
+    value = natoms * world * args.steps / dev_s
+    if args.lean:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "ms_per_step": dev_s / args.steps * 1e3,
+                              "stage_ms": stage_ms, "counters": counters, "lean": True}), flush=True)
+        pot.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---------------- e2e: pinned host buffers, copies inside every step
+    Zh = torch.from_numpy(Z).pin_memory()
+    posh = torch.from_numpy(pos).pin_memory()
+    Eh = torch.zeros(nstruct, dtype=torch.float64).pin_memory()
+    Fh = torch.zeros(natoms * 3, dtype=torch.float64).pin_memory()
+    Lh = torch.zeros(nstruct * 9, dtype=torch.float64).pin_memory()
+
+    def step_host():
+        code = L.hdnnp_eval_batch(
+            pot._c, nstruct, off.ctypes.data_as(C.POINTER(C.c_int64)),
+            C.cast(C.c_void_p(Zh.data_ptr()), C.POINTER(C.c_int32)),
+            C.cast(C.c_void_p(posh.data_ptr()), C.POINTER(C.c_double)), per.ctypes.data_as(C.POINTER(C.c_int32)),
+            latf.ctypes.data_as(C.POINTER(C.c_double)), C.cast(C.c_void_p(Eh.data_ptr()), C.POINTER(C.c_double)),
+            C.cast(C.c_void_p(Fh.data_ptr()), C.POINTER(C.c_double)),
+            C.cast(C.c_void_p(Lh.data_ptr()), C.POINTER(C.c_double)))
+        engine._check(code)
+
+    for _ in range(max(1, args.warmup // 2)):
+        step_host()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_host()  # synchronous: returns after the D2H copies completed
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    e2e = natoms * world * args.steps / e2e_s
+    h2d = Z.nbytes + pos.nbytes
+    d2h = Eh.numel() * 8 + Fh.numel() * 8 + Lh.numel() * 8
+
+    # ---------------- roofline of the dominant kernel
+    evals = max(counters["evaluations"], 1)
+    dom = max(("sf_values", "sf_gradients"), key=lambda k: stage_ms[k])
+    dom_ms = stage_ms[dom] / evals
+    flops = kernel_flops(dom, counters, evals)
+    peaks = measured_peaks(torch) if rank == 0 else {}
+    peak_key = "fp64" if args.precision == "fp64" else "fp32"
+    achieved = flops / (dom_ms / 1e3) / 1e12
+    roof = {"bound": peak_key, "kernel": dom, "achieved": achieved, "peak": peaks.get(peak_key),
+            "unit": "TFLOP/s", "frac": achieved / peaks[peak_key] if peaks.get(peak_key) else None,
+            "peak_source": f"measured in this run: cuBLAS {peak_key.upper()} GEMM (no TF32), best of 5",
+            "traffic": None,
+            "flops_per_launch": flops, "ms_per_launch": dom_ms,
+            "stage_ms_per_step": {k: v / evals for k, v in stage_ms.items()},
+            "units_per_step": {k: v / evals for k, v in counters.items() if k != "evaluations"}}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        cpu = cpu_baseline(structs, args.cpu_sample) if world == 1 else None
+        line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32+fp16",
+                "data": "synthetic (seeded ABX3 supercells, random-init 280-SF potential)",
+                "config": {"workload": f"batched mixed sizes: {nstruct} periodic ABX3 supercells per GPU "
+                                       f"(12-768 atoms, {natoms} atoms, seed 4+rank), E+F+stress",
+                           "global_batch": natoms * world, "precision": args.precision,
+                           "parallelism": f"replicas x{world} (independent structures per GPU)",
+                           "l2": "256 MB buffer written between timed steps; working set (G alone "
+                                 f"{natoms * 280 * 8 / 1e9:.1f} GB) is larger than L2"},
+                "e2e": {"value": e2e, "unit": "atom-steps/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": launches_per_step * args.steps,
+                "roofline": roof, "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    pot.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

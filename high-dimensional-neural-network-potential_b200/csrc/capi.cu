@@ -1,0 +1,723 @@
+// capi.cu -- C ABI of the engine (include/hdnnp_gpu.h): model upload,
+// evaluation contexts, host-side structure set-up and the stage pipeline.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hdnnp_gpu.h"
+#include "engine.h"
+#include "model.h"
+
+namespace hdnnp {
+size_t mlp_smem_bytes(const DevModel& m);
+}
+
+using namespace hdnnp;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(HDNNP_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+// ------------------------------------------------------------------ 3x3 helpers
+// column-major 3x3: a[r + 3c]
+double det3(const double* a) {
+    return a[0] * a[4] * a[8] + a[3] * a[7] * a[2] + a[6] * a[1] * a[5] - a[0] * a[7] * a[5] - a[3] * a[1] * a[8] -
+           a[6] * a[4] * a[2];
+}
+
+// inverse by adjugate / determinant (inv3DM, linalg.f90:264)
+void inv3(const double* a, double* b) {
+    auto A = [&](int r, int c) { return a[r + 3 * c]; };
+    double d = det3(a);
+    double r0[3] = {A(0, 0), A(0, 1), A(0, 2)}, r1[3] = {A(1, 0), A(1, 1), A(1, 2)}, r2[3] = {A(2, 0), A(2, 1), A(2, 2)};
+    double c0[3] = {r1[1] * r2[2] - r1[2] * r2[1], r0[2] * r2[1] - r0[1] * r2[2], r0[1] * r1[2] - r0[2] * r1[1]};
+    double c1[3] = {r1[2] * r2[0] - r1[0] * r2[2], r0[0] * r2[2] - r0[2] * r2[0], r0[2] * r1[0] - r0[0] * r1[2]};
+    double c2[3] = {r1[0] * r2[1] - r1[1] * r2[0], r0[1] * r2[0] - r0[0] * r2[1], r0[0] * r1[1] - r0[1] * r1[0]};
+    for (int k = 0; k < 3; ++k) {
+        b[0 + 3 * k] = c0[k] / d;
+        b[1 + 3 * k] = c1[k] / d;
+        b[2 + 3 * k] = c2[k] / d;
+    }
+}
+
+// getNcells (pointsets.f90:220-243)
+void n_cells(const double* lat, double cut, int* n) {
+    auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1];
+        c[1] = a[2] * b[0] - a[0] * b[2];
+        c[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double axb[3], axc[3], bxc[3];
+    cross(lat, lat + 3, axb);
+    cross(lat, lat + 6, axc);
+    cross(lat + 3, lat + 6, bxc);
+    for (double* v : {axb, axc, bxc}) {
+        double s = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; ++k) v[k] /= s;
+    }
+    double p0 = lat[0] * bxc[0] + lat[1] * bxc[1] + lat[2] * bxc[2];
+    double p1 = lat[3] * axc[0] + lat[4] * axc[1] + lat[5] * axc[2];
+    double p2 = lat[6] * axb[0] + lat[7] * axb[1] + lat[8] * axb[2];
+    n[0] = (int)std::ceil(cut / std::fabs(p0));
+    n[1] = (int)std::ceil(cut / std::fabs(p1));
+    n[2] = (int)std::ceil(cut / std::fabs(p2));
+}
+
+// Grid set-up of buildNeighborListGrid (neighborLists.f90:129-169).
+int struct_setup(int nat, const double* pos, int periodic, const double* lat, double rc, StructInfo& S) {
+    std::memset(&S, 0, sizeof S);
+    S.periodic = periodic ? 1 : 0;
+    if (nat <= 0) return fail(HDNNP_E_INPUT, "structure without atoms");
+    // host positions are checked here; device-resident ones by the wrap kernel
+    if (pos)
+        for (int i = 0; i < 3 * nat; ++i)
+            if (!std::isfinite(pos[i])) return fail(HDNNP_E_INPUT, "non-finite position");
+    if (!pos && !periodic) return fail(HDNNP_E_INPUT, "a molecule needs host positions for its bounding box");
+    if (periodic) {
+        std::memcpy(S.h, lat, sizeof S.h);
+        for (int k = 0; k < 9; ++k)
+            if (!std::isfinite(lat[k])) return fail(HDNNP_E_INPUT, "non-finite lattice");
+        double d = det3(S.h);
+        if (!(std::fabs(d) > 1e-12)) return fail(HDNNP_E_INPUT, "singular lattice");
+    } else {
+        for (int d = 0; d < 3; ++d) {
+            double mn = pos[d], mx = pos[d];
+            for (int i = 1; i < nat; ++i) {
+                mn = std::min(mn, pos[3 * i + d]);
+                mx = std::max(mx, pos[3 * i + d]);
+            }
+            S.org[d] = mn - 1.e-4;
+            double ext = 0.0;
+            for (int i = 0; i < nat; ++i) ext = std::max(ext, pos[3 * i + d] - S.org[d]);
+            S.h[d + 3 * d] = ext + 1.e-4;
+        }
+    }
+    inv3(S.h, S.hinv);
+    const double target = rc * 0.6;
+    double grid[9];
+    long long ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+        double len = std::sqrt(S.h[3 * d] * S.h[3 * d] + S.h[3 * d + 1] * S.h[3 * d + 1] + S.h[3 * d + 2] * S.h[3 * d + 2]);
+        S.ngrid[d] = (int)(len / target) + 1;
+        ncell *= S.ngrid[d];
+    }
+    // Very sparse molecules: coarsen the grid (same neighbour set, other order).
+    const long long limit = 64LL * nat + 4096;
+    while (ncell > limit) {
+        ncell = 1;
+        for (int d = 0; d < 3; ++d) {
+            S.ngrid[d] = std::max(1, S.ngrid[d] / 2);
+            ncell *= S.ngrid[d];
+        }
+    }
+    for (int d = 0; d < 3; ++d)
+        for (int r = 0; r < 3; ++r) grid[r + 3 * d] = S.h[r + 3 * d] / S.ngrid[d];
+    n_cells(grid, rc, S.nsearch);
+    if (periodic) {
+        int nl[3];
+        n_cells(S.h, rc, nl);
+        if (nl[0] > 100 || nl[1] > 100 || nl[2] > 100)
+            return fail(HDNNP_E_CAPACITY, "cell too small for the cutoff (more than 100 images per direction)");
+    }
+    for (int d = 0; d < 3; ++d)
+        if (S.nsearch[d] > 64) return fail(HDNNP_E_CAPACITY, "cell too skewed for the cell-list search");
+    return HDNNP_OK;
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t n) {
+        if (n <= cap && p) return HDNNP_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        size_t want = std::max<size_t>(n + n / 4, 64);
+        if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) {
+            cap = 0;
+            return fail(HDNNP_E_CUDA, "cudaMalloc of the workspace failed");
+        }
+        cap = want;
+        return HDNNP_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct hdnnp_model {
+    HostModel host;
+    DevModel dev;
+    int device = 0;
+    void* dmem = nullptr;
+};
+
+struct hdnnp_ctx {
+    hdnnp_model* model = nullptr;
+    cudaStream_t stream = nullptr;
+    int precision = HDNNP_PREC_FP64;
+    int launches = 0;
+    // device buffers
+    DevBuf<StructInfo> info;
+    DevBuf<int> Z, sid, elem, cell_of, cell_cnt, cell_start, cell_atoms, nei_cnt, nei_off, nei_j, nei_s, nei_rev,
+        el_count, el_start, el_atoms, scan_tmp, status;
+    DevBuf<double> pos, wpos, G, dEdG, atE, gent, gself, vir, force, energy, dEdLat;
+    // profiling: events around each stage, accumulated stage times and counters
+    bool profile = false;
+    bool prof_pending = false;
+    cudaEvent_t ev[8] = {};
+    double stage_ms[8] = {0};
+    long long host_counts[2] = {0, 0};
+    DevBuf<unsigned long long> stats;
+    // pinned host staging
+    int* h_status = nullptr;
+    Batch last{};
+    bool have_last = false;
+    std::vector<StructInfo> hinfo;
+    ~hdnnp_ctx() {
+        for (auto* b : {&Z, &sid, &elem, &cell_of, &cell_cnt, &cell_start, &cell_atoms, &nei_cnt, &nei_off, &nei_j,
+                        &nei_s, &nei_rev, &el_count, &el_start, &el_atoms, &scan_tmp, &status})
+            b->release();
+        for (auto* b : {&pos, &wpos, &G, &dEdG, &atE, &gent, &gself, &vir, &force, &energy, &dEdLat}) b->release();
+        info.release();
+        stats.release();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (h_status) cudaFreeHost(h_status);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// Build device tables from the parsed model.
+int upload_model(hdnnp_model* m) {
+    const HostModel& H = m->host;
+    DevModel& D = m->dev;
+    std::memset(&D, 0, sizeof D);
+    const int nel = (int)H.el.size();
+    if (nel > kMaxEl) return fail(HDNNP_E_CAPACITY, "too many elements");
+    D.nel = nel;
+    D.max_rc = H.max_rc;
+    for (int z = 0; z < 120; ++z) D.z2e[z] = (z <= kMaxZ) ? H.z2e[z] : -1;
+    int nsf_max = 0;
+    for (auto& e : H.el) nsf_max = std::max(nsf_max, (int)e.sfs.size());
+    D.nsf_max = nsf_max;
+    int nblk = 0;
+    for (int a = 0; a < nel; ++a)
+        for (int b = a; b < nel; ++b) {
+            D.blk_a[nblk] = a;
+            D.blk_b[nblk] = b;
+            ++nblk;
+        }
+    D.nblk = nblk;
+    std::vector<double> rc(nel), smean((size_t)nel * nsf_max, 0.0), swidth((size_t)nel * nsf_max, 1.0), ae(nel);
+    std::vector<int> nsf(nel), g2_off, g4_off;
+    std::vector<SF2> g2;
+    std::vector<SF4> g4;
+    int gmax = 1;
+    for (int c = 0; c < nel; ++c) {
+        const auto& E = H.el[c];
+        rc[c] = E.sfs[0].rcut;
+        nsf[c] = (int)E.sfs.size();
+        ae[c] = E.atom_energy;
+        for (int s = 0; s < nsf[c]; ++s) {
+            if (H.centersf) smean[(size_t)c * nsf_max + s] = E.sfs[s].smean;
+            if (H.scalesf) swidth[(size_t)c * nsf_max + s] = E.sfs[s].smax - E.sfs[s].smin;
+        }
+        for (int ne = 0; ne < nel; ++ne) {
+            g2_off.push_back((int)g2.size());
+            for (int s = 0; s < nsf[c]; ++s) {
+                const SymFn& f = E.sfs[s];
+                if (f.type == 2 && f.z1 == H.el[ne].z) g2.push_back(SF2{s, ne, f.eta, f.rs});
+            }
+        }
+        for (int t = 0; t < nblk; ++t) {
+            g4_off.push_back((int)g4.size());
+            const int za = H.el[D.blk_a[t]].z, zb = H.el[D.blk_b[t]].z;
+            std::vector<SF4> grp;
+            for (int s = 0; s < nsf[c]; ++s) {
+                const SymFn& f = E.sfs[s];
+                if (f.type != 3) continue;
+                if (!((f.z1 == za && f.z2 == zb) || (f.z1 == zb && f.z2 == za))) continue;
+                SF4 q;
+                q.sf = s;
+                int iz = (int)f.zeta;
+                q.izeta = (std::fabs(f.zeta - iz) < 1e-10 && iz >= 1) ? iz : -1;
+                q.eta = f.eta;
+                q.lambda = f.lambda;
+                q.zeta = f.zeta;
+                q.pf = q.izeta >= 1 ? std::ldexp(1.0, 1 - iz) : std::pow(2.0, 1.0 - f.zeta);
+                grp.push_back(q);
+            }
+            std::stable_sort(grp.begin(), grp.end(), [](const SF4& x, const SF4& y) { return x.eta < y.eta; });
+            gmax = std::max(gmax, (int)grp.size());
+            g4.insert(g4.end(), grp.begin(), grp.end());
+        }
+    }
+    g2_off.push_back((int)g2.size());
+    g4_off.push_back((int)g4.size());
+    D.gmax = gmax;
+
+    // networks: all elements share the hidden widths (global_nodes_short)
+    const int L = (int)H.el[0].net.size();
+    if (L > kMaxLayers) return fail(HDNNP_E_CAPACITY, "too many layers");
+    D.nlayers = L;
+    for (int l = 0; l < L; ++l) {
+        D.width[l + 1] = H.el[0].net[l].nout;
+        D.act[l] = H.el[0].net[l].act;
+    }
+    D.width[0] = nsf_max;
+    std::vector<double> w, wt, bias;
+    std::vector<long long> w_off, b_off;
+    for (int c = 0; c < nel; ++c) {
+        D.nin_el[c] = nsf[c];
+        for (int l = 0; l < L; ++l) {
+            const Layer& ly = H.el[c].net[l];
+            w_off.push_back((long long)w.size());
+            b_off.push_back((long long)bias.size());
+            w.insert(w.end(), ly.w.begin(), ly.w.end());
+            for (int i = 0; i < ly.nin; ++i)
+                for (int o = 0; o < ly.nout; ++o) wt.push_back(ly.w[(size_t)o * ly.nin + i]);
+            bias.insert(bias.end(), ly.b.begin(), ly.b.end());
+        }
+    }
+    // one device allocation for all tables
+    struct Part {
+        size_t off;
+        const void* src;
+        size_t bytes;
+    };
+    std::vector<Part> parts;
+    size_t off = 0;
+    auto add = [&](const void* src, size_t bytes) {
+        size_t o = off;
+        parts.push_back({o, src, bytes});
+        off += (std::max<size_t>(bytes, 8) + 255) & ~size_t(255);
+        return o;
+    };
+    size_t o_rc = add(rc.data(), rc.size() * 8), o_nsf = add(nsf.data(), nsf.size() * 4),
+           o_g2o = add(g2_off.data(), g2_off.size() * 4), o_g2 = add(g2.data(), g2.size() * sizeof(SF2)),
+           o_g4o = add(g4_off.data(), g4_off.size() * 4), o_g4 = add(g4.data(), g4.size() * sizeof(SF4)),
+           o_sm = add(smean.data(), smean.size() * 8), o_sw = add(swidth.data(), swidth.size() * 8),
+           o_w = add(w.data(), w.size() * 8), o_wt = add(wt.data(), wt.size() * 8), o_b = add(bias.data(), bias.size() * 8),
+           o_wo = add(w_off.data(), w_off.size() * 8), o_bo = add(b_off.data(), b_off.size() * 8),
+           o_ae = add(ae.data(), ae.size() * 8);
+    CUDA_TRY(cudaSetDevice(m->device));
+    CUDA_TRY(cudaMalloc(&m->dmem, off));
+    char* base = (char*)m->dmem;
+    for (auto& p : parts)
+        if (p.src && p.bytes) CUDA_TRY(cudaMemcpy(base + p.off, p.src, p.bytes, cudaMemcpyHostToDevice));
+    D.rc = (const double*)(base + o_rc);
+    D.nsf = (const int*)(base + o_nsf);
+    D.g2_off = (const int*)(base + o_g2o);
+    D.g2 = (const SF2*)(base + o_g2);
+    D.g4_off = (const int*)(base + o_g4o);
+    D.g4 = (const SF4*)(base + o_g4);
+    D.smean = (const double*)(base + o_sm);
+    D.swidth = (const double*)(base + o_sw);
+    D.w = (const double*)(base + o_w);
+    D.wt = (const double*)(base + o_wt);
+    D.b = (const double*)(base + o_b);
+    D.w_off = (const long long*)(base + o_wo);
+    D.b_off = (const long long*)(base + o_bo);
+    D.atom_energy = (const double*)(base + o_ae);
+    return HDNNP_OK;
+}
+
+int check_status(hdnnp_ctx* c) {
+    int f = c->h_status[0];
+    if (f & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
+    if (f & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
+    if (f & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
+    if (f & 8) return fail(HDNNP_E_INPUT, "non-finite position");
+    return HDNNP_OK;
+}
+
+int collect_profile(hdnnp_ctx* c) {
+    if (!c->prof_pending) return HDNNP_OK;
+    CUDA_TRY(cudaEventSynchronize(c->ev[7]));
+    for (int k = 0; k < 7; ++k) {
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]));
+        c->stage_ms[k] += ms;
+    }
+    c->prof_pending = false;
+    return HDNNP_OK;
+}
+
+// Core pipeline; inputs already on the device in c->Z / c->pos (or external
+// device pointers), structure set-up in c->hinfo.
+int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const double* posd, double* energy_d,
+                 double* force_d, double* dEdLat_d, cudaStream_t st) {
+    hdnnp_model* m = c->model;
+    const DevModel& D = m->dev;
+    int ncells = 0;
+    for (auto& S : c->hinfo) {
+        S.cell_off = ncells;
+        ncells += S.ngrid[0] * S.ngrid[1] * S.ngrid[2];
+    }
+    int r;
+    if ((r = c->info.ensure(nstruct))) return r;
+    CUDA_TRY(cudaMemcpyAsync(c->info.p, c->hinfo.data(), sizeof(StructInfo) * nstruct, cudaMemcpyHostToDevice, st));
+    const size_t N = natoms;
+    if ((r = c->sid.ensure(N)) || (r = c->elem.ensure(N)) || (r = c->wpos.ensure(3 * N)) || (r = c->cell_of.ensure(N)) ||
+        (r = c->cell_cnt.ensure(ncells + 1)) || (r = c->cell_start.ensure(ncells + 1)) ||
+        (r = c->cell_atoms.ensure(N)) || (r = c->nei_cnt.ensure(N + 1)) || (r = c->nei_off.ensure(N + 1)) ||
+        (r = c->el_count.ensure(kMaxEl + 1)) || (r = c->el_start.ensure(kMaxEl + 1)) || (r = c->el_atoms.ensure(N)) ||
+        (r = c->scan_tmp.ensure(std::max<size_t>(N, ncells) / 1024 + 256)) || (r = c->status.ensure(4)) ||
+        (r = c->G.ensure(N * D.nsf_max)) || (r = c->dEdG.ensure(N * D.nsf_max)) || (r = c->atE.ensure(N)) ||
+        (r = c->gself.ensure(3 * N)) || (r = c->vir.ensure(9 * N)))
+        return r;
+    if (!c->h_status) CUDA_TRY(cudaMallocHost(&c->h_status, 4 * sizeof(int)));
+    Batch b{};
+    b.nstruct = nstruct;
+    b.natoms = natoms;
+    b.ncells = ncells;
+    b.info = c->info.p;
+    b.Z = Zd;
+    b.pos = posd;
+    b.sid = c->sid.p;
+    b.elem = c->elem.p;
+    b.wpos = c->wpos.p;
+    b.cell_of = c->cell_of.p;
+    b.cell_cnt = c->cell_cnt.p;
+    b.cell_start = c->cell_start.p;
+    b.cell_atoms = c->cell_atoms.p;
+    b.nei_cnt = c->nei_cnt.p;
+    b.nei_off = c->nei_off.p;
+    b.el_count = c->el_count.p;
+    b.el_start = c->el_start.p;
+    b.el_atoms = c->el_atoms.p;
+    b.scan_tmp = c->scan_tmp.p;
+    b.status = c->status.p;
+    b.G = c->G.p;
+    b.dEdG = c->dEdG.p;
+    b.atE = c->atE.p;
+    b.gself = c->gself.p;
+    b.vir = c->vir.p;
+    b.force = force_d;
+    b.energy = energy_d;
+    b.dEdLat = dEdLat_d;
+    int L = 0;
+    if (c->profile) {
+        if ((r = collect_profile(c))) return r;
+        for (auto& e : c->ev)
+            if (!e) CUDA_TRY(cudaEventCreate(&e));
+        if (!c->stats.p) {
+            if ((r = c->stats.ensure(8))) return r;
+            CUDA_TRY(cudaMemset(c->stats.p, 0, 8 * sizeof(unsigned long long)));
+        }
+        b.stats = c->stats.p;
+        c->host_counts[0] += 1;
+        c->host_counts[1] += natoms;
+    }
+    auto mark = [&](int k) -> int {
+        if (c->profile) CUDA_TRY(cudaEventRecord(c->ev[k], st));
+        return HDNNP_OK;
+    };
+    CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
+    if ((r = mark(0))) return r;
+    L += launch_neighbour_build_a(b, D, st);
+    // entry total and the largest count
+    int tot_max[2];
+    CUDA_TRY(cudaMemcpyAsync(c->h_status + 2, b.nei_off + natoms, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(c->h_status + 3, b.status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if ((r = check_status(c))) return r;
+    tot_max[0] = c->h_status[2];
+    tot_max[1] = c->h_status[3];
+    if (tot_max[0] < 0) return fail(HDNNP_E_CAPACITY, "more than 2^31 neighbour entries");
+    const size_t E = (size_t)tot_max[0];
+    if ((r = c->nei_j.ensure(E + 1)) || (r = c->nei_s.ensure(E + 1)) || (r = c->nei_rev.ensure(E + 1)) ||
+        (r = c->gent.ensure(3 * E + 3)))
+        return r;
+    b.nentries = (int)E;
+    b.mmax = tot_max[1];
+    b.nei_j = c->nei_j.p;
+    b.nei_s = c->nei_s.p;
+    b.nei_rev = c->nei_rev.p;
+    b.gent = c->gent.p;
+    {
+        int mm = ((b.mmax + 31) / 32) * 32;
+        if (sf_smem_per_warp(mm, true) * 4 > 220 * 1024)
+            return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");
+        if (mlp_smem_bytes(D) > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+    }
+    if ((r = mark(1))) return r;  // after the host read: stage 1 starts here
+    L += launch_neighbour_build_b(b, D, st);
+    if ((r = mark(2))) return r;
+    L += launch_element_groups(b, D, st);
+    if ((r = mark(3))) return r;
+    L += launch_sf_values(b, D, st);
+    if ((r = mark(4))) return r;
+    L += launch_mlp(b, D, st);
+    if ((r = mark(5))) return r;
+    L += launch_sf_gradients(b, D, st);
+    if ((r = mark(6))) return r;
+    L += launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
+    if ((r = mark(7))) return r;
+    if (c->profile) c->prof_pending = true;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    c->launches = L;
+    c->last = b;
+    c->have_last = true;
+    return HDNNP_OK;
+}
+
+int prepare_structs(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* Z, const double* pos,
+                    const int32_t* periodic, const double* lat, bool validate_Z) {
+    const HostModel& H = c->model->host;
+    c->hinfo.resize(nstruct);
+    if (off[0] != 0) return fail(HDNNP_E_INPUT, "atom_off[0] must be 0");
+    for (int s = 0; s < nstruct; ++s) {
+        int64_t a0 = off[s], a1 = off[s + 1];
+        if (a1 <= a0) return fail(HDNNP_E_INPUT, "structure " + std::to_string(s) + " has no atoms");
+        if (a1 > INT32_MAX) return fail(HDNNP_E_CAPACITY, "more than 2^31 atoms");
+        int per = periodic ? periodic[s] : 0;
+        int r = struct_setup((int)(a1 - a0), pos ? pos + 3 * a0 : nullptr, per, lat + 9 * s, H.max_rc, c->hinfo[s]);
+        if (r) return fail(r, "structure " + std::to_string(s) + ": " + g_err);
+        c->hinfo[s].atom_off = (int)a0;
+        c->hinfo[s].nat = (int)(a1 - a0);
+    }
+    if (validate_Z)
+        for (int64_t i = 0; i < off[nstruct]; ++i)
+            if (Z[i] < 1 || Z[i] > kMaxZ || H.z2e[Z[i]] < 0)
+                return fail(HDNNP_E_INPUT, "atom " + std::to_string(i) + " has element Z=" + std::to_string(Z[i]) +
+                                               " that is not in the potential");
+    return HDNNP_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* hdnnp_last_error(void) { return g_err.c_str(); }
+
+int hdnnp_model_load_runner(const char* path, int device, hdnnp_model** out) {
+    if (!path || !out) return fail(HDNNP_E_INPUT, "null argument");
+    *out = nullptr;
+    auto* m = new hdnnp_model();
+    m->device = device;
+    std::string err;
+    if (!load_runner(path, m->host, err)) {
+        delete m;
+        return fail(HDNNP_E_IO, err);
+    }
+    int r = upload_model(m);
+    if (r) {
+        if (m->dmem) cudaFree(m->dmem);
+        delete m;
+        return r;
+    }
+    *out = m;
+    return HDNNP_OK;
+}
+
+int hdnnp_model_info(const hdnnp_model* m, int* nelem, int* Z, int* nsf, double* max_rc) {
+    if (!m) return fail(HDNNP_E_INPUT, "null model");
+    if (nelem) *nelem = (int)m->host.el.size();
+    for (size_t e = 0; e < m->host.el.size(); ++e) {
+        if (Z) Z[e] = m->host.el[e].z;
+        if (nsf) nsf[e] = (int)m->host.el[e].sfs.size();
+    }
+    if (max_rc) *max_rc = m->host.max_rc;
+    return HDNNP_OK;
+}
+
+void hdnnp_model_free(hdnnp_model* m) {
+    if (!m) return;
+    if (m->dmem) {
+        cudaSetDevice(m->device);
+        cudaFree(m->dmem);
+    }
+    delete m;
+}
+
+int hdnnp_ctx_create(hdnnp_model* m, hdnnp_ctx** out) {
+    if (!m || !out) return fail(HDNNP_E_INPUT, "null argument");
+    CUDA_TRY(cudaSetDevice(m->device));
+    auto* c = new hdnnp_ctx();
+    c->model = m;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(HDNNP_E_CUDA, "cudaStreamCreate failed");
+    }
+    *out = c;
+    return HDNNP_OK;
+}
+
+void hdnnp_ctx_free(hdnnp_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->model->device);
+    cudaStreamSynchronize(c->stream);
+    delete c;
+}
+
+int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision) {
+    if (!c) return fail(HDNNP_E_INPUT, "null context");
+    if (precision != HDNNP_PREC_FP64 && precision != HDNNP_PREC_MIXED) return fail(HDNNP_E_INPUT, "unknown precision");
+    c->precision = precision;
+    return HDNNP_OK;
+}
+
+int hdnnp_eval_batch(hdnnp_ctx* c, int nstruct, const int64_t* atom_off, const int32_t* Z, const double* pos,
+                     const int32_t* periodic, const double* lat, double* energy, double* force, double* dEdLat) {
+    if (!c || nstruct <= 0 || !atom_off || !Z || !pos || !lat || !energy || !force)
+        return fail(HDNNP_E_INPUT, "null argument or empty batch");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    if (dEdLat && periodic) {
+        // dEdLat rows of molecules are written as zeros
+    }
+    int r = prepare_structs(c, nstruct, atom_off, Z, pos, periodic, lat, true);
+    if (r) return r;
+    const int natoms = (int)atom_off[nstruct];
+    const size_t N = natoms;
+    cudaStream_t st = c->stream;
+    if ((r = c->Z.ensure(N)) || (r = c->pos.ensure(3 * N)) || (r = c->force.ensure(3 * N)) ||
+        (r = c->energy.ensure(nstruct)) || (r = c->dEdLat.ensure(9 * (size_t)nstruct)))
+        return r;
+    CUDA_TRY(cudaMemcpyAsync(c->Z.p, Z, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    r = run_pipeline(c, nstruct, natoms, c->Z.p, c->pos.p, c->energy.p, c->force.p, dEdLat ? c->dEdLat.p : nullptr, st);
+    if (r) return r;
+    CUDA_TRY(cudaMemcpyAsync(energy, c->energy.p, sizeof(double) * nstruct, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(force, c->force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (dEdLat) CUDA_TRY(cudaMemcpyAsync(dEdLat, c->dEdLat.p, sizeof(double) * 9 * nstruct, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return check_status(c);
+}
+
+int hdnnp_eval_batch_device(hdnnp_ctx* c, int nstruct, const int64_t* atom_off_host, const int64_t* atom_off_dev,
+                            const int32_t* Z_dev, const double* pos_dev, const int32_t* periodic_host,
+                            const double* lat_host, double* energy_dev, double* force_dev, double* dEdLat_dev,
+                            void* stream) {
+    (void)atom_off_dev;
+    if (!c || nstruct <= 0 || !atom_off_host || !Z_dev || !pos_dev || !lat_host || !energy_dev || !force_dev)
+        return fail(HDNNP_E_INPUT, "null argument or empty batch");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    // molecules need their bounding box: only periodic structures are allowed here
+    for (int s = 0; s < nstruct; ++s)
+        if (!periodic_host || !periodic_host[s])
+            return fail(HDNNP_E_INPUT, "hdnnp_eval_batch_device: all structures must be periodic");
+    int r = prepare_structs(c, nstruct, atom_off_host, nullptr, nullptr, periodic_host, lat_host, false);
+    if (r) return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    r = run_pipeline(c, nstruct, (int)atom_off_host[nstruct], Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st);
+    if (r) return r;
+    return HDNNP_OK;
+}
+
+int hdnnp_energy_and_forces(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, int periodic,
+                            const double* lat, double* energy, double* force, double* dEdLat) {
+    if (dEdLat && !periodic) return fail(HDNNP_E_INPUT, "dEdLat needs a periodic structure");
+    int64_t off[2] = {0, nat};
+    int32_t per = periodic ? 1 : 0;
+    double dummy[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    return hdnnp_eval_batch(c, 1, off, Z, pos, &per, lat ? lat : dummy, energy, force, dEdLat);
+}
+
+int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stress) {
+    if (!lat || !dEdLat || !stress) return fail(HDNNP_E_INPUT, "null argument");
+    double d = det3(lat);
+    if (d == 0.0) return fail(HDNNP_E_INPUT, "singular lattice");
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 3; ++k) s += dEdLat[i + 3 * k] * lat[j + 3 * k];
+            stress[i + 3 * j] = -1.0 / d * s;
+        }
+    return HDNNP_OK;
+}
+
+int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes) {
+    if (!c || !what || !host) return fail(HDNNP_E_INPUT, "null argument");
+    if (!c->have_last) return fail(HDNNP_E_STATE, "no evaluation yet");
+    const Batch& b = c->last;
+    const void* src = nullptr;
+    size_t n = 0;
+    std::string w(what);
+    int tmp = 0;
+    if (w == "G") { src = b.G; n = sizeof(double) * (size_t)b.natoms * c->model->dev.nsf_max; }
+    else if (w == "dEdG") { src = b.dEdG; n = sizeof(double) * (size_t)b.natoms * c->model->dev.nsf_max; }
+    else if (w == "atom_energy") { src = b.atE; n = sizeof(double) * b.natoms; }
+    else if (w == "nei_count") { src = b.nei_cnt; n = sizeof(int) * b.natoms; }
+    else if (w == "nei_offset") { src = b.nei_off; n = sizeof(int) * (b.natoms + 1); }
+    else if (w == "nei_index") { src = b.nei_j; n = sizeof(int) * b.nentries; }
+    else if (w == "nei_shift") { src = b.nei_s; n = sizeof(int) * b.nentries; }
+    else if (w == "nei_rev") { src = b.nei_rev; n = sizeof(int) * b.nentries; }
+    else if (w == "nsf_max") { tmp = c->model->dev.nsf_max; n = sizeof(int); }
+    else if (w == "nentries") { tmp = b.nentries; n = sizeof(int); }
+    else return fail(HDNNP_E_INPUT, "unknown item " + w);
+    if (bytes < n) return fail(HDNNP_E_CAPACITY, "buffer too small");
+    if (!src) {
+        std::memcpy(host, &tmp, n);
+        return HDNNP_OK;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpy(host, src, n, cudaMemcpyDeviceToHost));
+    return HDNNP_OK;
+}
+
+int hdnnp_ctx_set_profiling(hdnnp_ctx* c, int on) {
+    if (!c) return fail(HDNNP_E_INPUT, "null context");
+    c->profile = on != 0;
+    return HDNNP_OK;
+}
+
+int hdnnp_profile_read(hdnnp_ctx* c, double* stage_ms, int64_t* counters, int reset) {
+    if (!c) return fail(HDNNP_E_INPUT, "null context");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    int r = collect_profile(c);
+    if (r) return r;
+    unsigned long long dc[8] = {0};
+    if (c->stats.p) {
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        CUDA_TRY(cudaMemcpy(dc, c->stats.p, sizeof dc, cudaMemcpyDeviceToHost));
+    }
+    if (stage_ms)
+        for (int k = 0; k < 8; ++k) stage_ms[k] = k < 7 ? c->stage_ms[k] : 0.0;
+    if (counters) {
+        counters[0] = c->host_counts[0];
+        counters[1] = c->host_counts[1];
+        for (int k = 2; k < 8; ++k) counters[k] = (int64_t)dc[k];
+    }
+    if (reset) {
+        for (auto& x : c->stage_ms) x = 0.0;
+        c->host_counts[0] = c->host_counts[1] = 0;
+        if (c->stats.p) CUDA_TRY(cudaMemset(c->stats.p, 0, 8 * sizeof(unsigned long long)));
+    }
+    return HDNNP_OK;
+}
+
+int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches) {
+    if (!c || !launches) return fail(HDNNP_E_INPUT, "null argument");
+    *launches = c->launches;
+    return HDNNP_OK;
+}
+
+}  // extern "C"

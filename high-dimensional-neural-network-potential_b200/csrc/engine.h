@@ -1,0 +1,145 @@
+// engine.h -- device data layout and kernel launchers of the HDNNP engine.
+//
+// One evaluation of a batch of structures runs these stages on one stream:
+//   K1 wrap_and_bin     fractional wrap (FP64, h^-1 of each structure) + cell id
+//   K2 cell lists       counting sort of atoms into the cells of their structure
+//   K3 neighbours       per-atom count -> scan -> fill (CSR), reverse-entry index
+//   K4 sf_values        G2/G4 values, centred and scaled          (pass 1)
+//   K5 mlp              per-element network forward + dE/dG       (grouped by element)
+//   K6 sf_gradients     dE/dG-weighted G derivatives per neighbour entry (pass 2)
+//   K7 force_gather     F_a = -(g_self(a) + sum of reverse entries), deterministic
+//   K8 struct_reduce    compensated energy sum, virial -> dE/dh (FP64)
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace hdnnp {
+
+constexpr int kMaxEl = 16;
+
+// Per-structure set-up computed on the host in FP64 (same formulas as the
+// reference: artificial box for molecules, grid of >= 0.6 rc cells, search
+// range getNcells(grid, rc)).
+struct StructInfo {
+    double h[9];      // column-major lattice used for wrapping and image shifts
+    double hinv[9];   // its inverse (adjugate / det)
+    double org[3];    // box origin for molecules (0 for periodic cells)
+    int ngrid[3];     // cells per lattice direction
+    int nsearch[3];   // neighbouring cells searched per direction
+    int periodic;
+    int cell_off;     // first cell of this structure in the global cell arrays
+    int atom_off;     // first atom
+    int nat;
+};
+
+// Radial SF entry, grouped by (centre element, neighbour element).
+struct SF2 {
+    int sf;      // index in the centre element's SF list
+    int nel;     // neighbour element index
+    double eta, rs;
+};
+
+// Angular SF entry, grouped by (centre element, unordered element pair),
+// ordered by eta inside each group (one exp per distinct eta and pair).
+struct SF4 {
+    int sf;
+    int izeta;   // zeta if it is an integer (|zeta - int| < 1e-10), else -1
+    double eta, lambda, zeta, pf;  // pf = 2^(1-zeta)
+};
+
+// Device copy of the potential (pointers into one device allocation).
+struct DevModel {
+    int nel;
+    int nsf_max;
+    int nblk;                 // nel*(nel+1)/2 unordered element pairs
+    int gmax;                 // largest angular group
+    double max_rc;
+    int z2e[120];
+    int blk_a[kMaxEl * (kMaxEl + 1) / 2];
+    int blk_b[kMaxEl * (kMaxEl + 1) / 2];
+    const double* rc;         // [nel] cutoff of each centre element
+    const int* nsf;           // [nel]
+    const int* g2_off;        // [nel*nel+1]
+    const SF2* g2;
+    const int* g4_off;        // [nel*nblk+1]
+    const SF4* g4;
+    const double* smean;      // [nel*nsf_max] (0 when not centring)
+    const double* swidth;     // [nel*nsf_max] (1 when not scaling)
+    // networks
+    int nlayers;
+    int width[9];             // width[0] = input (per element: nsf), width[l+1] = out of layer l
+    char act[8];
+    int nin_el[kMaxEl];       // input width per element
+    const double* w;          // per element, per layer: W row-major [nout][nin]
+    const double* wt;         // same, transposed [nin][nout]
+    const double* b;
+    const long long* w_off;   // [nel*nlayers] offset of each layer's W / WT
+    const long long* b_off;   // [nel*nlayers]
+    const double* atom_energy;// [nel]
+};
+
+// Workspace pointers for one batch evaluation (all device memory).
+struct Batch {
+    int nstruct;
+    int natoms;
+    int ncells;
+    int nentries;             // neighbour entries (excluding the atoms themselves)
+    int mmax;                 // largest neighbour count of one atom
+    const StructInfo* info;   // [nstruct]
+    const int* Z;             // [natoms]
+    const double* pos;        // [3*natoms]
+    int* sid;                 // [natoms] structure of each atom
+    int* elem;                // [natoms] element index
+    double* wpos;             // [3*natoms] wrapped positions
+    int* cell_of;             // [natoms]
+    int* cell_cnt;            // [ncells+1]
+    int* cell_start;          // [ncells+1]
+    int* cell_atoms;          // [natoms]
+    int* nei_cnt;             // [natoms+1]
+    int* nei_off;             // [natoms+1]
+    int* nei_j;               // [nentries]
+    int* nei_s;               // [nentries] packed image shift
+    int* nei_rev;             // [nentries]
+    double* G;                // [natoms*nsf_max]
+    double* dEdG;             // [natoms*nsf_max]
+    double* atE;              // [natoms]
+    double* gent;             // [3*nentries]
+    double* gself;            // [3*natoms]
+    double* vir;              // [9*natoms]
+    double* force;            // [3*natoms]
+    double* energy;           // [nstruct]
+    double* dEdLat;           // [9*nstruct] or null
+    int* el_count;            // [nel+1]
+    int* el_start;            // [nel+1]
+    int* el_atoms;            // [natoms] atoms grouped by element
+    int* scan_tmp;            // scan block sums
+    int* status;              // [4] device error flags
+    unsigned long long* stats;  // [8] work counters or null
+};
+
+// packed image shift: three signed 8-bit lattice multiples
+__host__ __device__ inline int pack_shift(int x, int y, int z) {
+    return (x & 0xff) | ((y & 0xff) << 8) | ((z & 0xff) << 16);
+}
+__host__ __device__ inline void unpack_shift(int p, int& x, int& y, int& z) {
+    x = (int)(signed char)(p & 0xff);
+    y = (int)(signed char)((p >> 8) & 0xff);
+    z = (int)(signed char)((p >> 16) & 0xff);
+}
+
+// ------------------------------------------------------------------ launchers
+// Each returns the number of kernel launches it issued.
+int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s);  // wrap, bin, count
+int launch_scan(int* data, int n, int* tmp, int* total_out_dev, cudaStream_t s);   // exclusive scan in place, total in data[n]
+int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s);  // fill + reverse
+int launch_sf_values(const Batch& b, const DevModel& m, cudaStream_t s);
+int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s);
+int launch_sf_gradients(const Batch& b, const DevModel& m, cudaStream_t s);
+int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s);
+int launch_element_groups(const Batch& b, const DevModel& m, cudaStream_t s);
+
+size_t sf_smem_per_warp(int mmax, bool grad);
+
+}  // namespace hdnnp

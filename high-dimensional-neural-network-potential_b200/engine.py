@@ -1,0 +1,234 @@
+"""Python mirror of the reference's potential API over the C ABI.
+
+``Hdnnp`` stands for ``type(hdnnp)`` plus its routines in
+src/potentials/hdnnps.f90:
+
+=============================  ==============================================
+reference (Fortran)            here
+=============================  ==============================================
+parseRuNNerInput(h, path)      ``Hdnnp.from_runner(path)``       (:34)
+hdnnpEnergyAndForces(h, ats,   ``h.energy_and_forces(ats, dEdLat=True)``
+  energy, force, dEdLat)        -> (energy, force(nat,3), dEdLat(3,3)) (:333)
+type atStruct                  ``AtStruct``         (atomicStructure.f90:17)
+dEdLat2Stress(lat, dEdLat, s)  ``dEdLat_to_stress`` (atomicStructure.f90:679)
+=============================  ==============================================
+
+Errors that make the reference ``stop`` raise ``HdnnpError`` here.  Arrays
+follow the reference layout: ``ats[:, i]`` would be the Fortran column of atom
+i; in numpy we take ``pos`` of shape (nat, 3) (same memory order as the
+Fortran (3, nat) array) and ``lat`` of shape (3, 3) with ``lat[:, c]`` =
+lattice vector c.
+
+The compute path is ``lib/libhdnnp_b200.so``; if it is missing or cannot be
+loaded every call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libhdnnp_b200.so")
+
+HDNNP_PREC_FP64 = 0
+HDNNP_PREC_MIXED = 1
+
+_lib = None
+
+
+class HdnnpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hdnnp error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads libhdnnp_b200.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HdnnpError(-1, f"{LIB_PATH} is missing: build it with build.py (no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    P, D, I, I64 = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    L.hdnnp_last_error.restype = C.c_char_p
+    L.hdnnp_model_load_runner.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+    L.hdnnp_model_info.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), D]
+    L.hdnnp_model_free.argtypes = [P]
+    L.hdnnp_model_free.restype = None
+    L.hdnnp_ctx_create.argtypes = [P, C.POINTER(C.c_void_p)]
+    L.hdnnp_ctx_free.argtypes = [P]
+    L.hdnnp_ctx_free.restype = None
+    L.hdnnp_ctx_set_precision.argtypes = [P, C.c_int]
+    L.hdnnp_energy_and_forces.argtypes = [P, C.c_int, I, D, C.c_int, D, D, D, D]
+    L.hdnnp_eval_batch.argtypes = [P, C.c_int, I64, I, D, I, D, D, D, D]
+    L.hdnnp_eval_batch_device.argtypes = [P, C.c_int, I64, P, P, P, I, D, P, P, P, P]
+    L.hdnnp_dEdLat_to_stress.argtypes = [D, D, D]
+    L.hdnnp_debug_fetch.argtypes = [P, C.c_char_p, P, C.c_size_t]
+    L.hdnnp_last_launch_count.argtypes = [P, C.POINTER(C.c_int)]
+    L.hdnnp_ctx_set_profiling.argtypes = [P, C.c_int]
+    L.hdnnp_profile_read.argtypes = [P, D, I64, C.c_int]
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != 0:
+        raise HdnnpError(code, lib().hdnnp_last_error().decode())
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+@dataclass
+class AtStruct:
+    """type atStruct (atomicStructure.f90:17-28), prediction fields only."""
+
+    el: np.ndarray                      # atomic numbers (nat,)
+    ats: np.ndarray                     # positions (nat, 3), Bohr
+    lat: Optional[np.ndarray] = None    # (3, 3), lat[:, c] = lattice vector c
+    periodic: bool = field(default=False)
+
+    def __post_init__(self):
+        self.el = np.ascontiguousarray(self.el, dtype=np.int32)
+        self.ats = np.ascontiguousarray(self.ats, dtype=np.float64).reshape(-1, 3)
+        if self.lat is not None:
+            self.lat = np.asarray(self.lat, dtype=np.float64).reshape(3, 3)
+            self.periodic = True if self.periodic is False else self.periodic
+
+    @property
+    def nat(self) -> int:
+        return len(self.el)
+
+
+def _lat_flat(lat):
+    if lat is None:
+        return np.eye(3).ravel(order="F").copy()
+    return np.asarray(lat, dtype=np.float64).ravel(order="F").copy()
+
+
+class Hdnnp:
+    """A potential on one GPU with one evaluation context."""
+
+    def __init__(self, model_handle, device: int):
+        self._m = model_handle
+        self.device = device
+        ctx = C.c_void_p()
+        _check(lib().hdnnp_ctx_create(self._m, C.byref(ctx)))
+        self._c = ctx
+        n = C.c_int()
+        zs = (C.c_int * 128)()
+        ns = (C.c_int * 128)()
+        rc = C.c_double()
+        _check(lib().hdnnp_model_info(self._m, C.byref(n), zs, ns, C.byref(rc)))
+        self.elements = [zs[i] for i in range(n.value)]
+        self.nsf = {zs[i]: ns[i] for i in range(n.value)}
+        self.max_rc = rc.value
+        self.precision = HDNNP_PREC_FP64
+
+    @classmethod
+    def from_runner(cls, path: str, device: int = 0) -> "Hdnnp":
+        """parseRuNNerInput (hdnnps.f90:34)."""
+        h = C.c_void_p()
+        _check(lib().hdnnp_model_load_runner(os.fsencode(path), int(device), C.byref(h)))
+        return cls(h, device)
+
+    def close(self):
+        if getattr(self, "_c", None):
+            lib().hdnnp_ctx_free(self._c)
+            self._c = None
+        if getattr(self, "_m", None):
+            lib().hdnnp_model_free(self._m)
+            self._m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, mode: int):
+        _check(lib().hdnnp_ctx_set_precision(self._c, int(mode)))
+        self.precision = mode
+
+    # ------------------------------------------------------------------ evaluation
+    def energy_and_forces(self, ats: AtStruct, dEdLat: bool = False):
+        """hdnnpEnergyAndForces (hdnnps.f90:333): energy, forces (nat,3),
+        and dE/dh (3,3) when ``dEdLat`` (periodic structures only)."""
+        n = ats.nat
+        E = C.c_double()
+        F = np.zeros((n, 3))
+        dl = np.zeros(9) if dEdLat else None
+        _check(lib().hdnnp_energy_and_forces(
+            self._c, n, _ip(ats.el), _dp(ats.ats), 1 if ats.periodic else 0,
+            _dp(_lat_flat(ats.lat)), C.byref(E), _dp(F), _dp(dl)))
+        return E.value, F, (dl.reshape(3, 3, order="F") if dl is not None else None)
+
+    def eval_batch(self, structs: Sequence[dict], dEdLat: bool = True):
+        """Independent structures in one batch (dicts with Z, pos, lat)."""
+        off = np.zeros(len(structs) + 1, np.int64)
+        off[1:] = np.cumsum([len(s["Z"]) for s in structs])
+        Z = np.ascontiguousarray(np.concatenate([s["Z"] for s in structs]), dtype=np.int32)
+        pos = np.ascontiguousarray(np.concatenate([s["pos"] for s in structs]), dtype=np.float64)
+        lat = np.concatenate([_lat_flat(s["lat"]) for s in structs])
+        per = np.array([0 if s["lat"] is None else 1 for s in structs], np.int32)
+        return self.eval_batch_arrays(off, Z, pos, per, lat, dEdLat)
+
+    def eval_batch_arrays(self, off, Z, pos, per, lat_flat, dEdLat=True, out=None):
+        ns = len(off) - 1
+        if out is None:
+            out = {"energy": np.zeros(ns), "forces": np.zeros((int(off[-1]), 3)),
+                   "dEdLat": np.zeros(9 * ns) if dEdLat else None}
+        _check(lib().hdnnp_eval_batch(
+            self._c, ns, off.ctypes.data_as(C.POINTER(C.c_int64)), _ip(Z), _dp(pos), _ip(per), _dp(lat_flat),
+            _dp(out["energy"]), _dp(out["forces"]), _dp(out["dEdLat"])))
+        return out
+
+    STAGES = ("neighbour_count", "neighbour_fill", "element_groups", "sf_values", "mlp", "sf_gradients",
+              "force_reduce")
+    COUNTERS = ("evaluations", "atoms", "entries", "cand_pairs", "pairs", "g4_terms", "g2_terms")
+
+    def set_profiling(self, on: bool = True):
+        _check(lib().hdnnp_ctx_set_profiling(self._c, 1 if on else 0))
+
+    def profile(self, reset: bool = False):
+        ms = np.zeros(8)
+        cnt = np.zeros(8, np.int64)
+        _check(lib().hdnnp_profile_read(self._c, _dp(ms), cnt.ctypes.data_as(C.POINTER(C.c_int64)), 1 if reset else 0))
+        return dict(zip(self.STAGES, ms[:7].tolist())), dict(zip(self.COUNTERS, cnt[:7].tolist()))
+
+    def launches(self) -> int:
+        n = C.c_int()
+        _check(lib().hdnnp_last_launch_count(self._c, C.byref(n)))
+        return n.value
+
+    def fetch(self, what: str, count: int, dtype=np.float64):
+        a = np.zeros(count, dtype=dtype)
+        _check(lib().hdnnp_debug_fetch(self._c, what.encode(), a.ctypes.data_as(C.c_void_p), a.nbytes))
+        return a
+
+
+def dEdLat_to_stress(lat, dEdLat):
+    """dEdLat2Stress (atomicStructure.f90:679): stress = -1/det(h) dEdLat h^T."""
+    out = np.zeros(9)
+    L = np.asarray(lat, dtype=np.float64).ravel(order="F").copy()
+    dl = np.asarray(dEdLat, dtype=np.float64).ravel(order="F").copy()
+    _check(lib().hdnnp_dEdLat_to_stress(_dp(L), _dp(dl), _dp(out)))
+    return out.reshape(3, 3, order="F")
+
+
+def exported_symbols(header: str):
+    """Function names declared in a C header (for the load test)."""
+    import re
+
+    txt = open(header).read()
+    return sorted(set(re.findall(r"\b(hdnnp_[a-z0-9_]+)\s*\(", txt)))

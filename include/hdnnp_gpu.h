@@ -1,0 +1,142 @@
+/* hdnnp_gpu.h -- C ABI of the B200-native HDNNP prediction engine.
+ *
+ * Drop-in boundary for the reference's Fortran potential API
+ * (Jonas-Finkler/High-Dimensional-Neural-Network-Potential,
+ * src/potentials/hdnnps.f90).  Every call is plain C: pointers, sizes and
+ * status codes; no CUDA or C++ types appear in the signatures (streams are
+ * passed as void*).  A Fortran ISO_C_BINDING binding of these entry points is
+ * in fortran/hdnnps_gpu.f90.
+ *
+ * Conventions (same as the reference):
+ *   positions   double[3*nat]  x,y,z per atom, Bohr      (atStruct%ats(3,nat))
+ *   lattice     double[9]      column-major 3x3, column c = lattice vector c
+ *                                                        (atStruct%lat(3,3))
+ *   Z           int32[nat]     atomic numbers           (atStruct%el)
+ *   forces      double[3*nat]  -dE/dr
+ *   dEdLat      double[9]      dE/dh (column-major, like lat); periodic only
+ *   energy      double         sum of atomic NN outputs + atom_energy
+ * Energies come out in the units of the potential (the reference converts
+ * nothing, atomicStructure.f90:157).
+ *
+ * All entry points return HDNNP_OK (0) or an error code; they never abort.
+ * hdnnp_last_error() returns a message for the calling thread.
+ */
+#ifndef HDNNP_GPU_H
+#define HDNNP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HDNNP_OK = 0,
+    HDNNP_E_INPUT = 1,    /* bad argument, unknown element, singular cell ...  */
+    HDNNP_E_IO = 2,       /* a RuNNer file is missing or malformed             */
+    HDNNP_E_CAPACITY = 3, /* a size limit of the engine is exceeded            */
+    HDNNP_E_TIMEOUT = 4,  /* a bounded wait expired                            */
+    HDNNP_E_CUDA = 5,     /* a CUDA runtime call failed                        */
+    HDNNP_E_STATE = 6     /* call not valid in the current state               */
+} hdnnp_status;
+
+typedef enum {
+    HDNNP_PREC_FP64 = 0,  /* FP64 everywhere (parity form)                                  */
+    HDNNP_PREC_MIXED = 1  /* FP32 symmetry functions, FP16 tensor-core MLP with hi+lo split,
+                             FP64 wrapping, energy and virial reductions                      */
+} hdnnp_precision;
+
+typedef struct hdnnp_model hdnnp_model; /* parsed potential + its device copy */
+typedef struct hdnnp_ctx hdnnp_ctx;     /* evaluation context: stream + workspace */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* hdnnp_last_error(void);
+
+/* ---------------------------------------------------------------- model
+ * Replaces parseRuNNerInput(handle, path) (hdnnps.f90:34-233) together with
+ * sortSymFunctions (:235), readScaling (:269) and readWeights (:302).
+ * `path` is a directory; like the reference it is joined with the file names
+ * (a trailing '/' is added if missing).  Differences from the reference,
+ * which stops the process instead: errors are returned; there is no
+ * 200-symmetry-function cap (nmaxSFs, hdnnps.f90:48); symmetry-function types
+ * other than 2 and 3 are rejected instead of skipped.  The model is uploaded
+ * to `device` (CUDA ordinal).                                              */
+int hdnnp_model_load_runner(const char* path, int device, hdnnp_model** out);
+
+/* Elements (sorted by Z) and their symmetry-function counts; arrays of
+ * length >= 118.  max_rc = largest cutoff (hdnnp%maxRc, hdnnps.f90:16).    */
+int hdnnp_model_info(const hdnnp_model* m, int* nelem, int* Z, int* nsf, double* max_rc);
+
+void hdnnp_model_free(hdnnp_model* m);
+
+/* ---------------------------------------------------------------- context
+ * A context owns a CUDA stream and a growable device workspace.  It is used
+ * by one host thread at a time; several contexts may share one model.      */
+int hdnnp_ctx_create(hdnnp_model* m, hdnnp_ctx** out);
+void hdnnp_ctx_free(hdnnp_ctx* c);
+int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
+
+/* ---------------------------------------------------------------- evaluation
+ * Replaces hdnnpEnergyAndForces(handle, ats, energy, force, dEdLat)
+ * (hdnnps.f90:333-371): neighbour lists (hdnnpCalcNeighborLists :373),
+ * symmetry functions (hdnnpCalcSymfunctions :390) and the networks with the
+ * force/dEdLat contraction (hdnnpCalcNNs :487).  Host arrays in, host arrays
+ * out, synchronous.  dEdLat may be NULL; it requires periodic != 0 (the
+ * reference reads an uninitialised lattice otherwise, hdnnps.f90:509).     */
+int hdnnp_energy_and_forces(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, int periodic,
+                            const double* lat, double* energy, double* force, double* dEdLat);
+
+/* Batch of nstruct independent structures in CSR form (no reference
+ * counterpart: the reference evaluates one structure per call).
+ * atom_off[nstruct+1] (atom_off[0] = 0); Z, pos, force indexed by global
+ * atom; periodic[nstruct]; lat[9*nstruct]; energy[nstruct];
+ * dEdLat[9*nstruct] or NULL (rows of non-periodic structures are zero).    */
+int hdnnp_eval_batch(hdnnp_ctx* c, int nstruct, const int64_t* atom_off, const int32_t* Z, const double* pos,
+                     const int32_t* periodic, const double* lat, double* energy, double* force, double* dEdLat);
+
+/* Same, with every array already in device memory of the context's device
+ * (inputs resident in HBM; no host copies).  Asynchronous on `stream`
+ * (a cudaStream_t, or NULL for the context's own stream) except for one
+ * small device-to-host read of the neighbour-entry total.  atom_off_host is
+ * a HOST copy of the offsets (used to size the workspace).                  */
+int hdnnp_eval_batch_device(hdnnp_ctx* c, int nstruct, const int64_t* atom_off_host, const int64_t* atom_off_dev,
+                            const int32_t* Z_dev, const double* pos_dev, const int32_t* periodic_host,
+                            const double* lat_host, double* energy_dev, double* force_dev, double* dEdLat_dev,
+                            void* stream);
+
+/* ---------------------------------------------------------------- stress
+ * dEdLat2Stress (atomicStructure.f90:679-686): stress = -1/det(h) dEdLat h^T. */
+int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stress);
+
+/* ---------------------------------------------------------------- inspection
+ * Copies an intermediate of the last evaluation on `c` to host memory, for
+ * tests and profiling.  what: "G" (scaled symmetry functions, nat x nsf_max,
+ * row stride nsf_max), "dEdG" (same layout), "atom_energy" (nat),
+ * "nei_count" (nat, excluding the atom itself), "nei_index" (entries),
+ * "nei_shift" (entries, packed image shift), "nsf_max" (1 int).
+ * `bytes` is the size of `host`; returns HDNNP_E_CAPACITY if too small.     */
+int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes);
+
+/* Kernel launches issued by the last evaluation on `c`. */
+int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches);
+
+/* ---------------------------------------------------------------- profiling
+ * Tracing hook in place of the reference's per-stage cpu_time prints
+ * (hdnnps.f90:346-368), which are always on there.  With profiling enabled
+ * every evaluation records CUDA events around each stage on its stream and
+ * counts work units; the totals accumulate until reset.
+ * Stages (index): 0 neighbour count, 1 neighbour fill + reverse index,
+ * 2 element grouping, 3 symmetry-function values, 4 networks,
+ * 5 symmetry-function gradients, 6 force gather + structure reduction.
+ * Counters (index): 0 evaluations, 1 atoms, 2 neighbour entries,
+ * 3 candidate angular pairs, 4 contributing angular pairs (r_jk < rc),
+ * 5 angular SF terms, 6 radial SF terms.                                    */
+int hdnnp_ctx_set_profiling(hdnnp_ctx* c, int on);
+int hdnnp_profile_read(hdnnp_ctx* c, double* stage_ms /* [8] */, int64_t* counters /* [8] */, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HDNNP_GPU_H */

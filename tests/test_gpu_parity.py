@@ -1,0 +1,143 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle.
+
+Tolerances of the plain FP64 form: |dE| <= 1e-10 |E|, max |dF| <= 1e-9
+Ha/Bohr, max |d dEdLat| <= 1e-9 (and the same for the stress).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ABX3_DIR, EXAMPLE_DIR, GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+E_REL, F_ABS, L_ABS = 1e-10, 1e-9, 1e-9
+
+
+@pytest.fixture(scope="module")
+def eng(pkg):
+    from hdnnp_b200 import engine
+
+    return engine
+
+
+@pytest.fixture(scope="module")
+def gex(eng):
+    p = eng.Hdnnp.from_runner(EXAMPLE_DIR)
+    yield p
+    p.close()
+
+
+@pytest.fixture(scope="module")
+def gab(eng):
+    p = eng.Hdnnp.from_runner(ABX3_DIR)
+    yield p
+    p.close()
+
+
+def small_cell(W, seed=7, strain=0.05, jitter=0.15):
+    rng = np.random.default_rng(seed)
+    c = W.strain(W.abx3_cell(), rng.uniform(-strain, strain, (3, 3)))
+    c["pos"] = c["pos"] + rng.normal(0, jitter, c["pos"].shape)
+    return c
+
+
+def check(E, F, dl, ref):
+    assert abs(E - ref["energy"]) <= E_REL * abs(ref["energy"]), (E, ref["energy"])
+    assert np.abs(F - ref["forces"]).max() <= F_ABS, np.abs(F - ref["forces"]).max()
+    if dl is not None:
+        assert np.abs(dl - ref["dEdLat"]).max() <= L_ABS, np.abs(dl - ref["dEdLat"]).max()
+
+
+def test_example_molecule(eng, gex, ex_model, c1):
+    s = c1[0]
+    E, F, _ = gex.energy_and_forces(eng.AtStruct(s["Z"], s["pos"]))
+    check(E, F, None, ex_model.eval(s["Z"], s["pos"]))
+    fx = json.load(open(os.path.join(GOLDEN, "oracle_fixtures.json")))["c1"]
+    assert abs(E - fx["energy"]) <= E_REL * abs(fx["energy"])
+    assert np.abs(F - np.array(fx["forces"])).max() <= F_ABS
+
+
+def test_small_cell_images_and_stress(eng, gab, abx3_model, W, orc):
+    c = small_cell(W)
+    E, F, dl = gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], c["lat"]), dEdLat=True)
+    ref = abx3_model.eval(c["Z"], c["pos"], c["lat"])
+    check(E, F, dl, ref)
+    st = eng.dEdLat_to_stress(c["lat"], dl)
+    assert np.abs(st - orc.dEdLat_to_stress(c["lat"], ref["dEdLat"])).max() <= L_ABS
+    fx = json.load(open(os.path.join(GOLDEN, "oracle_fixtures.json")))["cell"]
+    assert abs(E - fx["energy"]) <= E_REL * abs(fx["energy"])
+
+
+def test_768_atoms(eng, gab, abx3_model, W):
+    s = W.config_c2()
+    E, F, dl = gab.energy_and_forces(eng.AtStruct(s["Z"], s["pos"], s["lat"]), dEdLat=True)
+    check(E, F, dl, abx3_model.eval(s["Z"], s["pos"], s["lat"]))
+
+
+def test_stage_outputs(eng, gab, abx3_model, W):
+    s = small_cell(W, seed=3)
+    gab.energy_and_forces(eng.AtStruct(s["Z"], s["pos"], s["lat"]), dEdLat=True)
+    n = len(s["Z"])
+    nsf = int(gab.fetch("nsf_max", 1, np.int32)[0])
+    G = gab.fetch("G", n * nsf).reshape(n, nsf)
+    Gref = abx3_model.symfunctions(s["Z"], s["pos"], s["lat"])
+    assert np.abs(G - Gref[:, :nsf]).max() <= 1e-11
+    ref = abx3_model.eval(s["Z"], s["pos"], s["lat"], per_atom=True)
+    dEdG = gab.fetch("dEdG", n * nsf).reshape(n, nsf)
+    assert np.abs(dEdG - ref["dEdG"][:, :nsf]).max() <= 1e-10
+    atE = gab.fetch("atom_energy", n)
+    assert np.abs(atE - ref["atom_energies"]).max() <= 1e-11
+    # neighbour sets (the oracle list includes the atom itself as entry 0)
+    cnt = gab.fetch("nei_count", n, np.int32)
+    oc, oidx, _ = abx3_model.neighbours(s["Z"], s["pos"], s["lat"])
+    assert (cnt == oc - 1).all()
+    nidx = gab.fetch("nei_index", int(cnt.sum()), np.int32)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    for i in range(n):
+        assert list(nidx[off[i]:off[i + 1]]) == list(oidx[i, 1:oc[i]])  # same order as the reference
+
+
+def test_batch_alone_equals_in_mix(eng, gab, W):
+    structs = W.config_c4(n_struct=24, seed=11)
+    mix = gab.eval_batch(structs, dEdLat=True)
+    off = np.concatenate([[0], np.cumsum([len(s["Z"]) for s in structs])])
+    for k in (0, 5, 17, 23):
+        alone = gab.eval_batch([structs[k]], dEdLat=True)
+        assert alone["energy"][0] == mix["energy"][k]
+        assert np.array_equal(alone["forces"], mix["forces"][off[k]:off[k + 1]])
+        assert np.array_equal(alone["dEdLat"], mix["dEdLat"][9 * k:9 * k + 9])
+
+
+def test_mixed_batch_vs_oracle(eng, gab, abx3_model, W):
+    structs = W.config_c4(n_struct=16, seed=12)
+    structs.append(W.read_xyz(os.path.join(EXAMPLE_DIR, "input.xyz")))  # a molecule in the batch
+    structs[-1]["Z"] = np.array([7, 6, 1, 1, 1, 1, 1, 1], np.int32)
+    out = gab.eval_batch(structs, dEdLat=True)
+    off = np.concatenate([[0], np.cumsum([len(s["Z"]) for s in structs])])
+    for k, s in enumerate(structs):
+        ref = abx3_model.eval(s["Z"], s["pos"], s["lat"])
+        dl = out["dEdLat"][9 * k:9 * k + 9].reshape(3, 3, order="F") if s["lat"] is not None else None
+        check(out["energy"][k], out["forces"][off[k]:off[k + 1]], dl, ref)
+
+
+def test_errors_are_status_codes(eng, gab, W):
+    c = small_cell(W)
+    bad = dict(c)
+    with pytest.raises(eng.HdnnpError, match="not in the potential"):
+        Z = c["Z"].copy()
+        Z[0] = 8
+        gab.energy_and_forces(eng.AtStruct(Z, c["pos"], c["lat"]))
+    with pytest.raises(eng.HdnnpError, match="singular"):
+        gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], np.zeros((3, 3)) + 1.0))
+    with pytest.raises(eng.HdnnpError, match="periodic"):
+        gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"]), dEdLat=True)
+    with pytest.raises(eng.HdnnpError, match="non-finite"):
+        p = c["pos"].copy()
+        p[2, 1] = np.nan
+        gab.energy_and_forces(eng.AtStruct(c["Z"], p, c["lat"]))
+    # the context stays usable after errors
+    E, F, _ = gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], c["lat"]))
+    assert np.isfinite(E)
