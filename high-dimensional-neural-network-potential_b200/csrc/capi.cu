@@ -721,3 +721,173 @@ int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches) {
 }
 
 }  // extern "C"
+
+// ====================================================================== no-allocation entry point
+// hdnnp_energy_and_forces_noalloc: the evaluation of hdnnp_energy_and_forces
+// for callers that cannot allocate GPU memory at evaluation time, such as a
+// host code that runs under a fixed memory budget handed out at start-up,
+// code running inside someone else's stream capture, or a language binding
+// without access to the CUDA allocator.  All intermediates live in one
+// static device array instead of a context workspace; inputs and outputs are
+// the caller's host arrays, as for hdnnp_energy_and_forces.
+#include <mutex>
+
+namespace {
+
+// Size of the static scratch.  Every GPU that loads the library's code for
+// this entry point keeps these bytes reserved until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host
+// code the symbol g_noalloc_scratch only names a host-side stand-in; a kernel
+// must be given this address instead.
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu[kNoAllocMaxDevices];
+
+int noalloc_setup(int dev) {
+    if (g_noalloc_ptr[dev]) return HDNNP_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return fail(HDNNP_E_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+    return HDNNP_OK;
+}
+
+// Bump carving of the static scratch (256-byte aligned regions).
+struct Carve {
+    unsigned char* base;
+    size_t used = 0;
+    bool over = false;
+    template <typename T>
+    T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        if (used + bytes > kNoAllocScratchBytes) {
+            over = true;
+            return nullptr;
+        }
+        T* p = (T*)(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+}  // namespace
+
+extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, const int32_t* Z, const double* pos,
+                                               int periodic, const double* lat, double* energy, double* force,
+                                               double* dEdLat) {
+    if (!m || nat <= 0 || !Z || !pos || !energy || !force) return fail(HDNNP_E_INPUT, "null argument or no atoms");
+    if (periodic && !lat) return fail(HDNNP_E_INPUT, "periodic structure without a lattice");
+    if (dEdLat && !periodic) return fail(HDNNP_E_INPUT, "dEdLat needs a periodic structure");
+    const int dev = m->device;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HDNNP_E_INPUT, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu[dev]);
+    CUDA_TRY(cudaSetDevice(dev));
+    int r = noalloc_setup(dev);
+    if (r) return r;
+    const HostModel& H = m->host;
+    const DevModel& D = m->dev;
+    for (int i = 0; i < nat; ++i)
+        if (Z[i] < 1 || Z[i] > kMaxZ || H.z2e[Z[i]] < 0)
+            return fail(HDNNP_E_INPUT, "atom " + std::to_string(i) + " has element Z=" + std::to_string(Z[i]) +
+                                           " that is not in the potential");
+    double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    StructInfo S;
+    r = struct_setup(nat, pos, periodic, periodic ? lat : ident, H.max_rc, S);
+    if (r) return r;
+    S.atom_off = 0;
+    S.nat = nat;
+    S.cell_off = 0;
+    const int ncells = S.ngrid[0] * S.ngrid[1] * S.ngrid[2];
+    const size_t N = nat;
+
+    Carve cv{g_noalloc_ptr[dev]};
+    Batch b{};
+    b.nstruct = 1;
+    b.natoms = nat;
+    b.ncells = ncells;
+    StructInfo* info = cv.take<StructInfo>(1);
+    int32_t* Zd = cv.take<int32_t>(N);
+    double* posd = cv.take<double>(3 * N);
+    b.sid = cv.take<int>(N);
+    b.elem = cv.take<int>(N);
+    b.wpos = cv.take<double>(3 * N);
+    b.cell_of = cv.take<int>(N);
+    b.cell_cnt = cv.take<int>(ncells + 1);
+    b.cell_start = cv.take<int>(ncells + 1);
+    b.cell_atoms = cv.take<int>(N);
+    b.nei_cnt = cv.take<int>(N + 1);
+    b.nei_off = cv.take<int>(N + 1);
+    b.el_count = cv.take<int>(kMaxEl + 1);
+    b.el_start = cv.take<int>(kMaxEl + 1);
+    b.el_atoms = cv.take<int>(N);
+    b.scan_tmp = cv.take<int>(std::max<size_t>(N, ncells) / 1024 + 256);
+    b.status = cv.take<int>(4);
+    b.G = cv.take<double>(N * D.nsf_max);
+    b.dEdG = cv.take<double>(N * D.nsf_max);
+    b.atE = cv.take<double>(N);
+    b.gself = cv.take<double>(3 * N);
+    b.vir = cv.take<double>(9 * N);
+    double* Fd = cv.take<double>(3 * N);
+    double* Ed = cv.take<double>(1);
+    double* Ld = cv.take<double>(9);
+    if (cv.over)
+        return fail(HDNNP_E_CAPACITY, "structure too large for the " + std::to_string(kNoAllocScratchBytes >> 20) +
+                                          " MiB static scratch of hdnnp_energy_and_forces_noalloc (" +
+                                          std::to_string(nat) + " atoms)");
+    b.info = info;
+    b.Z = Zd;
+    b.pos = posd;
+    b.force = Fd;
+    b.energy = Ed;
+    b.dEdLat = dEdLat ? Ld : nullptr;
+    b.stats = nullptr;
+    cudaStream_t st = 0;  // legacy default stream: nothing is created
+    CUDA_TRY(cudaMemcpy(info, &S, sizeof S, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(Zd, Z, sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(posd, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+    // the scratch keeps the previous call's contents: clear what must start at zero
+    CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
+    launch_neighbour_build_a(b, D, st);
+    int h[3] = {0, 0, 0};
+    CUDA_TRY(cudaMemcpy(&h[0], b.status, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&h[1], b.nei_off + nat, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&h[2], b.status + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h[0] & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
+    if (h[0] & 8) return fail(HDNNP_E_INPUT, "non-finite position");
+    const size_t E = (size_t)std::max(h[1], 0);
+    b.nentries = (int)E;
+    b.mmax = h[2];
+    b.nei_j = cv.take<int>(E + 1);
+    b.nei_s = cv.take<int>(E + 1);
+    b.nei_rev = cv.take<int>(E + 1);
+    b.gent = cv.take<double>(3 * E + 3);
+    if (cv.over)
+        return fail(HDNNP_E_CAPACITY, "too many neighbour entries (" + std::to_string(E) + ") for the " +
+                                          std::to_string(kNoAllocScratchBytes >> 20) +
+                                          " MiB static scratch of hdnnp_energy_and_forces_noalloc");
+    {
+        int mm = ((b.mmax + 31) / 32) * 32;
+        if (sf_smem_per_warp(mm, true) * 4 > 220 * 1024)
+            return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");
+        if (mlp_smem_bytes(D) > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+    }
+    launch_neighbour_build_b(b, D, st);
+    launch_element_groups(b, D, st);
+    launch_sf_values(b, D, st);
+    launch_mlp(b, D, st);
+    launch_sf_gradients(b, D, st);
+    launch_forces_and_reduce(b, D, dEdLat != nullptr, st);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpy(energy, Ed, sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(force, Fd, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
+    if (dEdLat) CUDA_TRY(cudaMemcpy(dEdLat, Ld, sizeof(double) * 9, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&h[0], b.status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h[0] & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
+    if (h[0] & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
+    return HDNNP_OK;
+}

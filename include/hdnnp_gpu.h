@@ -105,6 +105,33 @@ int hdnnp_eval_batch_device(hdnnp_ctx* c, int nstruct, const int64_t* atom_off_h
                             const double* lat_host, double* energy_dev, double* force_dev, double* dEdLat_dev,
                             void* stream);
 
+/* ---------------------------------------------------------------- no-allocation variant
+ * No counterpart in the reference.  The same evaluation as
+ * hdnnp_energy_and_forces (host arrays in and out, same arguments and
+ * results), for callers that cannot allocate GPU memory when they evaluate:
+ * an MD or Monte Carlo host code that runs under a fixed device-memory budget
+ * handed out at start-up, code that runs inside another library's stream
+ * capture (where cudaMalloc is not allowed), or a language binding without
+ * access to the CUDA allocator.  It needs no context and calls no cudaMalloc,
+ * cudaFree or allocating library routine: all intermediates live in one
+ * static 32 MiB device array compiled into the library, which every GPU that
+ * runs this entry point keeps reserved until the process exits.
+ * Limit: the structure must fit that array (for a 280-SF potential about
+ * 5,000 atoms with ~52 neighbours each; in general about
+ * nat * (16 * nsf_max + 210) + neighbour_entries * 36 bytes); larger inputs
+ * return HDNNP_E_CAPACITY with the size that did not fit.
+ * Set-up: the first call on a device looks up the device address of the
+ * static array (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.
+ * Sharing: every call uses the same array and it keeps the last call's
+ * contents (the call clears what must start at zero).  Calls are serialised
+ * per device inside one process; calls that overlap on the GPU from other
+ * processes or other copies of the library race on the array.  The work runs
+ * on the legacy default stream and the call returns when it is done.        */
+int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, const int32_t* Z, const double* pos,
+                                    int periodic, const double* lat, double* energy, double* force,
+                                    double* dEdLat);
+
 /* ---------------------------------------------------------------- stress
  * dEdLat2Stress (atomicStructure.f90:679-686): stress = -1/det(h) dEdLat h^T. */
 int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stress);
