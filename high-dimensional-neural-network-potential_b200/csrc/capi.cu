@@ -13,10 +13,6 @@
 #include "engine.h"
 #include "model.h"
 
-namespace hdnnp {
-size_t mlp_smem_bytes(const DevModel& m);
-}
-
 using namespace hdnnp;
 
 namespace {
@@ -177,12 +173,14 @@ struct hdnnp_ctx {
     hdnnp_model* model = nullptr;
     cudaStream_t stream = nullptr;
     int precision = HDNNP_PREC_FP64;
+    int generic_sf = 0;
     int launches = 0;
     // device buffers
     DevBuf<StructInfo> info;
     DevBuf<int> Z, sid, elem, cell_of, cell_cnt, cell_start, cell_atoms, nei_cnt, nei_off, nei_j, nei_s, nei_rev,
         el_count, el_start, el_atoms, scan_tmp, status;
     DevBuf<double> pos, wpos, G, dEdG, atE, gent, gself, vir, force, energy, dEdLat;
+    DevBuf<float> Gf, dEdGf, atEf, gentf, gselff, virf;  // mixed-precision intermediates
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -200,6 +198,7 @@ struct hdnnp_ctx {
                         &nei_s, &nei_rev, &el_count, &el_start, &el_atoms, &scan_tmp, &status})
             b->release();
         for (auto* b : {&pos, &wpos, &G, &dEdG, &atE, &gent, &gself, &vir, &force, &energy, &dEdLat}) b->release();
+        for (auto* b : {&Gf, &dEdGf, &atEf, &gentf, &gselff, &virf}) b->release();
         info.release();
         stats.release();
         for (auto& e : ev)
@@ -280,6 +279,80 @@ int upload_model(hdnnp_model* m) {
     g4_off.push_back((int)g4.size());
     D.gmax = gmax;
 
+    // Angular-SF grid for the fast kernels: distinct lambda, zeta, eta over
+    // all G4 SFs; every group must map one-to-one into lambda x zeta x eta.
+    std::vector<short> pmap;
+    {
+        std::vector<double> lams, zets, etas;
+        auto idx_of = [](std::vector<double>& v, double x) {
+            for (size_t i = 0; i < v.size(); ++i)
+                if (std::fabs(v[i] - x) <= 1e-12 * std::max(1.0, std::fabs(x))) return (int)i;
+            v.push_back(x);
+            return (int)v.size() - 1;
+        };
+        for (auto& E : H.el)
+            for (auto& f : E.sfs)
+                if (f.type == 3) {
+                    idx_of(lams, f.lambda);
+                    idx_of(zets, f.zeta);
+                    idx_of(etas, f.eta);
+                }
+        std::sort(zets.begin(), zets.end());
+        std::sort(etas.begin(), etas.end());
+        int shape = 0;
+        bool ints_ok = true;
+        int maxz = 1;
+        for (double z : zets) {
+            int iz = (int)z;
+            if (std::fabs(z - iz) < 1e-10 && iz >= 1) maxz = std::max(maxz, iz);
+            if (z > 31.0) ints_ok = false;
+        }
+        for (int id = 1; id <= 4 && ints_ok; ++id)
+            if ((int)lams.size() <= kFastShapes[id][0] && (int)zets.size() <= kFastShapes[id][1] &&
+                (int)etas.size() <= kFastShapes[id][2]) {
+                shape = id;
+                break;
+            }
+        if (!lams.empty() && shape) {
+            const int NL = kFastShapes[shape][0], NZ = kFastShapes[shape][1], NE = kFastShapes[shape][2];
+            const int P = NL * NZ * NE;
+            pmap.assign((size_t)nel * nblk * P, (short)-1);
+            bool ok = true;
+            for (int c = 0; c < nel && ok; ++c)
+                for (int t = 0; t < nblk && ok; ++t) {
+                    const int za = H.el[D.blk_a[t]].z, zb = H.el[D.blk_b[t]].z;
+                    for (int s = 0; s < nsf[c]; ++s) {
+                        const SymFn& f = H.el[c].sfs[s];
+                        if (f.type != 3 || !((f.z1 == za && f.z2 == zb) || (f.z1 == zb && f.z2 == za))) continue;
+                        const int l = idx_of(lams, f.lambda), z = idx_of(zets, f.zeta), e = idx_of(etas, f.eta);
+                        short& slot = pmap[((size_t)c * nblk + t) * P + (l * NZ + z) * NE + e];
+                        if (slot >= 0) ok = false;  // two SFs on one grid point: generic kernels
+                        slot = (short)s;
+                    }
+                }
+            if (ok) {
+                D.fast = shape;
+                D.fl = (int)lams.size();
+                D.fz = (int)zets.size();
+                D.fe = (int)etas.size();
+                for (int l = 0; l < D.fl; ++l) D.lam[l] = lams[l];
+                for (int z = 0; z < D.fz; ++z) {
+                    D.zet[z] = zets[z];
+                    const int iz = (int)zets[z];
+                    D.zint[z] = (std::fabs(zets[z] - iz) < 1e-10 && iz >= 1) ? iz - 1 : -1;
+                    D.pfz[z] = D.zint[z] >= 0 ? std::ldexp(1.0, -D.zint[z]) : std::pow(2.0, 1.0 - zets[z]);
+                }
+                for (int e = 0; e < D.fe; ++e) D.eta4[e] = etas[e];
+                int bit = 0;
+                while ((1 << (bit + 1)) <= maxz) ++bit;
+                D.zmaxbit = bit;
+            } else {
+                pmap.clear();
+            }
+        }
+        if (!D.fast) pmap.assign(1, (short)-1);
+    }
+
     // networks: all elements share the hidden widths (global_nodes_short)
     const int L = (int)H.el[0].net.size();
     if (L > kMaxLayers) return fail(HDNNP_E_CAPACITY, "too many layers");
@@ -324,6 +397,9 @@ int upload_model(hdnnp_model* m) {
            o_w = add(w.data(), w.size() * 8), o_wt = add(wt.data(), wt.size() * 8), o_b = add(bias.data(), bias.size() * 8),
            o_wo = add(w_off.data(), w_off.size() * 8), o_bo = add(b_off.data(), b_off.size() * 8),
            o_ae = add(ae.data(), ae.size() * 8);
+    std::vector<float> wf(w.begin(), w.end()), wtf(wt.begin(), wt.end()), bf(bias.begin(), bias.end());
+    size_t o_pm = add(pmap.data(), pmap.size() * sizeof(short)), o_wf = add(wf.data(), wf.size() * 4),
+           o_wtf = add(wtf.data(), wtf.size() * 4), o_bf = add(bf.data(), bf.size() * 4);
     CUDA_TRY(cudaSetDevice(m->device));
     CUDA_TRY(cudaMalloc(&m->dmem, off));
     char* base = (char*)m->dmem;
@@ -343,6 +419,10 @@ int upload_model(hdnnp_model* m) {
     D.w_off = (const long long*)(base + o_wo);
     D.b_off = (const long long*)(base + o_bo);
     D.atom_energy = (const double*)(base + o_ae);
+    D.pmap = (const short*)(base + o_pm);
+    D.wf = (const float*)(base + o_wf);
+    D.wtf = (const float*)(base + o_wtf);
+    D.bf = (const float*)(base + o_bf);
     return HDNNP_OK;
 }
 
@@ -460,24 +540,44 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.nei_s = c->nei_s.p;
     b.nei_rev = c->nei_rev.p;
     b.gent = c->gent.p;
+    // mixed precision runs on the fast (lambda x zeta x eta) kernels; potentials
+    // outside their shapes evaluate in FP64 with the generic kernels
+    const bool fast = D.fast && !c->generic_sf;
+    const bool mixed = c->precision == HDNNP_PREC_MIXED && fast;
+    if (mixed) {
+        if ((r = c->Gf.ensure(N * D.nsf_max)) || (r = c->dEdGf.ensure(N * D.nsf_max)) || (r = c->atEf.ensure(N)) ||
+            (r = c->gentf.ensure(3 * E + 3)) || (r = c->gselff.ensure(3 * N)) || (r = c->virf.ensure(9 * N)))
+            return r;
+        b.Gf = c->Gf.p;
+        b.dEdGf = c->dEdGf.p;
+        b.atEf = c->atEf.p;
+        b.gentf = c->gentf.p;
+        b.gselff = c->gselff.p;
+        b.virf = c->virf.p;
+    }
     {
         int mm = ((b.mmax + 31) / 32) * 32;
-        if (sf_smem_per_warp(mm, true) * 4 > 220 * 1024)
+        const size_t sf_smem =
+            fast ? sf_fast_smem_per_warp(mm, D.nsf_max, D.nblk, fast_shape_p(D.fast), true, mixed) * 4
+                   : sf_smem_per_warp(mm, true) * 4;
+        if (sf_smem > 220 * 1024 || (fast && mm > 1024))
             return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");
-        if (mlp_smem_bytes(D) > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+        if (mlp_smem_bytes(D, mixed ? sizeof(float) : sizeof(double)) > 220 * 1024)
+            return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
     }
     if ((r = mark(1))) return r;  // after the host read: stage 1 starts here
     L += launch_neighbour_build_b(b, D, st);
     if ((r = mark(2))) return r;
     L += launch_element_groups(b, D, st);
     if ((r = mark(3))) return r;
-    L += launch_sf_values(b, D, st);
+    L += fast ? launch_sf_values_fast(b, D, mixed, st) : launch_sf_values(b, D, st);
     if ((r = mark(4))) return r;
-    L += launch_mlp(b, D, st);
+    L += mixed ? launch_mlp_fp32(b, D, st) : launch_mlp(b, D, st);
     if ((r = mark(5))) return r;
-    L += launch_sf_gradients(b, D, st);
+    L += fast ? launch_sf_gradients_fast(b, D, mixed, st) : launch_sf_gradients(b, D, st);
     if ((r = mark(6))) return r;
-    L += launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
+    L += mixed ? launch_forces_and_reduce_fp32(b, D, dEdLat_d != nullptr, st)
+               : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
     if ((r = mark(7))) return r;
     if (c->profile) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
@@ -583,6 +683,15 @@ int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision) {
     if (precision != HDNNP_PREC_FP64 && precision != HDNNP_PREC_MIXED) return fail(HDNNP_E_INPUT, "unknown precision");
     c->precision = precision;
     return HDNNP_OK;
+}
+
+int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
+    if (!c || !name) return fail(HDNNP_E_INPUT, "null argument");
+    if (std::string(name) == "generic_sf") {
+        c->generic_sf = value != 0;
+        return HDNNP_OK;
+    }
+    return fail(HDNNP_E_INPUT, std::string("unknown option ") + name);
 }
 
 int hdnnp_eval_batch(hdnnp_ctx* c, int nstruct, const int64_t* atom_off, const int32_t* Z, const double* pos,
@@ -874,7 +983,7 @@ extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, co
         int mm = ((b.mmax + 31) / 32) * 32;
         if (sf_smem_per_warp(mm, true) * 4 > 220 * 1024)
             return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");
-        if (mlp_smem_bytes(D) > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+        if (mlp_smem_bytes(D, sizeof(double)) > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
     }
     launch_neighbour_build_b(b, D, st);
     launch_element_groups(b, D, st);

@@ -78,6 +78,24 @@ struct DevModel {
     const long long* w_off;   // [nel*nlayers] offset of each layer's W / WT
     const long long* b_off;   // [nel*nlayers]
     const double* atom_energy;// [nel]
+    // Angular-SF grid of the potential: the distinct lambda, zeta and eta of
+    // all G4 SFs.  When every (centre element, element pair) group maps
+    // one-to-one into the product lambda x zeta x eta of a compiled shape
+    // (NL, NZ, NE), the fast kernels evaluate per pair one power table and one
+    // exponential per eta and contract in that product space.
+    int fast;                 // 0: generic kernels; else the shape id (1..4)
+    int fl, fz, fe;           // model counts (<= NL, NZ, NE of the shape)
+    double lam[2];
+    double zet[8];
+    int zint[8];              // zeta - 1 if zeta is an integer >= 1, else -1
+    double pfz[8];            // 2^(1 - zeta)
+    double eta4[8];
+    int zmaxbit;              // highest bit of the integer zeta - 1 values
+    const short* pmap;        // [nel][nblk][P]: SF index of product entry p, or -1
+    // FP32 copies of the network weights (mixed-precision form)
+    const float* wf;
+    const float* wtf;
+    const float* bf;
 };
 
 // Workspace pointers for one batch evaluation (all device memory).
@@ -117,6 +135,13 @@ struct Batch {
     int* scan_tmp;            // scan block sums
     int* status;              // [4] device error flags
     unsigned long long* stats;  // [8] work counters or null
+    // FP32 intermediates of the mixed-precision form (same layouts)
+    float* Gf;
+    float* dEdGf;
+    float* atEf;
+    float* gentf;
+    float* gselff;
+    float* virf;
 };
 
 // packed image shift: three signed 8-bit lattice multiples
@@ -139,7 +164,19 @@ int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_sf_gradients(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s);
 int launch_element_groups(const Batch& b, const DevModel& m, cudaStream_t s);
+int launch_mlp_fp32(const Batch& b, const DevModel& m, cudaStream_t s);
+int launch_forces_and_reduce_fp32(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s);
+size_t mlp_smem_bytes(const DevModel& m, size_t elem);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
+
+// Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).
+constexpr int kFastShapes[5][3] = {{0, 0, 0}, {2, 2, 1}, {2, 4, 2}, {2, 4, 4}, {2, 8, 2}};
+inline int fast_shape_p(int id) { return kFastShapes[id][0] * kFastShapes[id][1] * kFastShapes[id][2]; }
+
+// Fast (product-space) symmetry-function kernels, FP64 (T = double) or FP32.
+int launch_sf_values_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t s);
+int launch_sf_gradients_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t s);
+size_t sf_fast_smem_per_warp(int mmax, int nsf, int nblk, int P, bool grad, bool fp32);
 
 }  // namespace hdnnp

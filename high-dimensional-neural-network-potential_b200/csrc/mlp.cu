@@ -26,15 +26,42 @@ __device__ __forceinline__ double act_f(char a, double x) {
         default: return x;
     }
 }
-// derivative from the pre-activation c and the activation y = act(c)
-__device__ __forceinline__ double act_d(char a, double c, double y) {
+__device__ __forceinline__ float act_f(char a, float x) {
     switch (a) {
-        case 't': return 1.0 - y * y;
-        case 'p': return 1.0 / (1.0 + exp(-1.0 * c));
-        case 'r': return c > 0.0 ? 1.0 : 0.0;
-        default: return 1.0;
+        case 't': return tanhf(x);
+        case 'p': return log1pf(expf(x));
+        case 'r': return x > 0.0f ? x : 0.0f;
+        default: return x;
     }
 }
+// derivative from the pre-activation c and the activation y = act(c)
+template <typename T>
+__device__ __forceinline__ T act_d(char a, T c, T y) {
+    switch (a) {
+        case 't': return (T)1 - y * y;
+        case 'p': return (T)1 / ((T)1 + (T)exp((double)-c));
+        case 'r': return c > (T)0 ? (T)1 : (T)0;
+        default: return (T)1;
+    }
+}
+
+template <typename T> struct MB;
+template <> struct MB<double> {
+    static __device__ const double* G(const Batch& b) { return b.G; }
+    static __device__ double* dEdG(const Batch& b) { return b.dEdG; }
+    static __device__ double* atE(const Batch& b) { return b.atE; }
+    static __device__ const double* w(const DevModel& m) { return m.w; }
+    static __device__ const double* wt(const DevModel& m) { return m.wt; }
+    static __device__ const double* bias(const DevModel& m) { return m.b; }
+};
+template <> struct MB<float> {
+    static __device__ const float* G(const Batch& b) { return b.Gf; }
+    static __device__ float* dEdG(const Batch& b) { return b.dEdGf; }
+    static __device__ float* atE(const Batch& b) { return b.atEf; }
+    static __device__ const float* w(const DevModel& m) { return m.wf; }
+    static __device__ const float* wt(const DevModel& m) { return m.wtf; }
+    static __device__ const float* bias(const DevModel& m) { return m.bf; }
+};
 
 __global__ void k_count_elements(Batch b, int nel) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -67,8 +94,10 @@ __global__ void k_fill_elements(Batch b) {
     }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_mlp(Batch b, DevModel m, int maxw) {
-    extern __shared__ __align__(16) double sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* sm = (T*)sm_raw;
     // locate (element, tile) of this block
     int tile = blockIdx.x, e = -1, t0 = 0, cnt = 0;
     for (int x = 0; x < m.nel; ++x) {
@@ -86,38 +115,39 @@ __global__ void __launch_bounds__(kThreads) k_mlp(Batch b, DevModel m, int maxw)
     const int nin = m.nin_el[e];
     const int L = m.nlayers;
     // shared layout: x[kTile][nin] | per layer c_l, y_l [kTile][w_l] | two delta buffers [kTile][maxw]
-    double* x = sm;
-    double* cbuf[8];
-    double* ybuf[8];
-    double* p = x + kTile * nin;
+    T* x = sm;
+    T* cbuf[8];
+    T* ybuf[8];
+    T* p = x + kTile * nin;
     for (int l = 0; l < L; ++l) {
         cbuf[l] = p;
         p += kTile * m.width[l + 1];
         ybuf[l] = p;
         p += kTile * m.width[l + 1];
     }
-    double* d0 = p;
-    double* d1 = p + kTile * maxw;
+    T* d0 = p;
+    T* d1 = p + kTile * maxw;
     const int tid = threadIdx.x;
+    const T* Gin = MB<T>::G(b);
     for (int idx = tid; idx < kTile * nin; idx += kThreads) {
         int a = idx / nin, i = idx % nin;
-        x[idx] = a < cnt ? b.G[(size_t)b.el_atoms[t0 + a] * m.nsf_max + i] : 0.0;
+        x[idx] = a < cnt ? Gin[(size_t)b.el_atoms[t0 + a] * m.nsf_max + i] : (T)0;
     }
     __syncthreads();
     // forward
-    const double* in = x;
+    const T* in = x;
     int win = nin;
     for (int l = 0; l < L; ++l) {
         const int wout = m.width[l + 1];
-        const double* WT = m.wt + m.w_off[e * L + l];
-        const double* bb = m.b + m.b_off[e * L + l];
+        const T* WT = MB<T>::wt(m) + m.w_off[e * L + l];
+        const T* bb = MB<T>::bias(m) + m.b_off[e * L + l];
         const char act = m.act[l];
         for (int idx = tid; idx < kTile * wout; idx += kThreads) {
             int a = idx / wout, o = idx % wout;
-            double s = 0.0;
-            const double* xa = in + a * win;
+            T s = (T)0;
+            const T* xa = in + a * win;
             for (int i = 0; i < win; ++i) s += WT[(size_t)i * wout + o] * xa[i];
-            double c = s + bb[o];
+            T c = s + bb[o];
             cbuf[l][idx] = c;
             ybuf[l][idx] = act_f(act, c);
         }
@@ -126,7 +156,8 @@ __global__ void __launch_bounds__(kThreads) k_mlp(Batch b, DevModel m, int maxw)
         win = wout;
     }
     // energy
-    for (int a = tid; a < cnt; a += kThreads) b.atE[b.el_atoms[t0 + a]] = ybuf[L - 1][a * m.width[L]] + m.atom_energy[e];
+    for (int a = tid; a < cnt; a += kThreads)
+        MB<T>::atE(b)[b.el_atoms[t0 + a]] = (T)((double)ybuf[L - 1][a * m.width[L]] + m.atom_energy[e]);
     // backward: delta of the output layer (gradOut = 1)
     {
         const int w = m.width[L];
@@ -134,25 +165,25 @@ __global__ void __launch_bounds__(kThreads) k_mlp(Batch b, DevModel m, int maxw)
             d0[idx] = act_d(m.act[L - 1], cbuf[L - 1][idx], ybuf[L - 1][idx]);
     }
     __syncthreads();
-    double* dcur = d0;
-    double* dnext = d1;
+    T* dcur = d0;
+    T* dnext = d1;
     for (int l = L - 1; l >= 0; --l) {
         const int wout = m.width[l + 1];
         const int wi = (l == 0) ? nin : m.width[l];
-        const double* W = m.w + m.w_off[e * L + l];
+        const T* W = MB<T>::w(m) + m.w_off[e * L + l];
         for (int idx = tid; idx < kTile * wi; idx += kThreads) {
             int a = idx / wi, i = idx % wi;
-            double s = 0.0;
-            const double* da = dcur + a * wout;
+            T s = (T)0;
+            const T* da = dcur + a * wout;
             for (int o = 0; o < wout; ++o) s += da[o] * W[(size_t)o * wi + i];
             if (l == 0) {
-                if (a < cnt) b.dEdG[(size_t)b.el_atoms[t0 + a] * m.nsf_max + i] = s;
+                if (a < cnt) MB<T>::dEdG(b)[(size_t)b.el_atoms[t0 + a] * m.nsf_max + i] = s;
             } else {
                 dnext[idx] = s * act_d(m.act[l - 1], cbuf[l - 1][idx], ybuf[l - 1][idx]);
             }
         }
         __syncthreads();
-        double* tmp = dcur;
+        T* tmp = dcur;
         dcur = dnext;
         dnext = tmp;
     }
@@ -169,7 +200,7 @@ int launch_element_groups(const Batch& b, const DevModel& m, cudaStream_t s) {
     return 3;
 }
 
-size_t mlp_smem_bytes(const DevModel& m) {
+size_t mlp_smem_bytes(const DevModel& m, size_t elem) {
     int nin = 0, maxw = 1;
     for (int e = 0; e < m.nel; ++e) nin = nin > m.nin_el[e] ? nin : m.nin_el[e];
     size_t n = (size_t)kTile * nin;
@@ -178,22 +209,28 @@ size_t mlp_smem_bytes(const DevModel& m) {
         if (m.width[l + 1] > maxw) maxw = m.width[l + 1];
     }
     n += 2 * (size_t)kTile * maxw;  // deltas of the hidden/output layers
-    return n * sizeof(double);
+    return n * elem;
 }
 
-int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
+template <typename T>
+void run_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
     int nin = 0, maxw = 1;
     for (int e = 0; e < m.nel; ++e) nin = nin > m.nin_el[e] ? nin : m.nin_el[e];
     for (int l = 0; l < m.nlayers; ++l)
         if (m.width[l + 1] > maxw) maxw = m.width[l + 1];
-    size_t smem = mlp_smem_bytes(m);
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
+    size_t smem = mlp_smem_bytes(m, sizeof(T));
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_mlp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int tiles = b.natoms / kTile + m.nel + 1;
-    k_mlp<<<tiles, kThreads, smem, s>>>(b, m, maxw);
+    k_mlp<T><<<tiles, kThreads, smem, s>>>(b, m, maxw);
+}
+
+int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
+    run_mlp<double>(b, m, s);
+    return 1;
+}
+
+int launch_mlp_fp32(const Batch& b, const DevModel& m, cudaStream_t s) {
+    run_mlp<float>(b, m, s);
     return 1;
 }
 

@@ -17,16 +17,17 @@ namespace hdnnp {
 
 namespace {
 
-__global__ void k_force_gather(Batch b) {
+template <typename T>
+__global__ void k_force_gather(Batch b, const T* gself, const T* gent) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= b.natoms) return;
-    double fx = b.gself[3 * (size_t)a], fy = b.gself[3 * (size_t)a + 1], fz = b.gself[3 * (size_t)a + 2];
+    double fx = gself[3 * (size_t)a], fy = gself[3 * (size_t)a + 1], fz = gself[3 * (size_t)a + 2];
     const int e0 = b.nei_off[a], e1 = b.nei_off[a + 1];
     for (int e = e0; e < e1; ++e) {
         const size_t r = (size_t)b.nei_rev[e];
-        fx += b.gent[3 * r];
-        fy += b.gent[3 * r + 1];
-        fz += b.gent[3 * r + 2];
+        fx += gent[3 * r];
+        fy += gent[3 * r + 1];
+        fz += gent[3 * r + 2];
     }
     b.force[3 * (size_t)a] = -fx;
     b.force[3 * (size_t)a + 1] = -fy;
@@ -52,7 +53,8 @@ struct KSum {
 
 constexpr int kRedThreads = 256;
 
-__global__ void __launch_bounds__(kRedThreads) k_struct_reduce(Batch b, int want_dEdLat) {
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_struct_reduce(Batch b, int want_dEdLat, const T* atE, const T* vir) {
     __shared__ double se[kRedThreads], sc[kRedThreads];
     __shared__ double sv[9][kRedThreads];
     const int st = blockIdx.x;
@@ -61,10 +63,10 @@ __global__ void __launch_bounds__(kRedThreads) k_struct_reduce(Batch b, int want
     KSum k{0.0, 0.0};
     double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = threadIdx.x; i < n; i += kRedThreads) {
-        k.add(b.atE[a0 + i]);
+        k.add((double)atE[a0 + i]);
         if (want_dEdLat)
 #pragma unroll
-            for (int u = 0; u < 9; ++u) v[u] += b.vir[9 * (size_t)(a0 + i) + u];
+            for (int u = 0; u < 9; ++u) v[u] += (double)vir[9 * (size_t)(a0 + i) + u];
     }
     se[threadIdx.x] = k.s;
     sc[threadIdx.x] = k.c;
@@ -106,8 +108,16 @@ __global__ void __launch_bounds__(kRedThreads) k_struct_reduce(Batch b, int want
 
 int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s) {
     (void)m;
-    k_force_gather<<<(b.natoms + 255) / 256, 256, 0, s>>>(b);
-    k_struct_reduce<<<b.nstruct, kRedThreads, 0, s>>>(b, want_dEdLat);
+    k_force_gather<double><<<(b.natoms + 255) / 256, 256, 0, s>>>(b, b.gself, b.gent);
+    k_struct_reduce<double><<<b.nstruct, kRedThreads, 0, s>>>(b, want_dEdLat, b.atE, b.vir);
+    return 2;
+}
+
+// mixed-precision form: FP32 intermediates, FP64 accumulation and outputs
+int launch_forces_and_reduce_fp32(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s) {
+    (void)m;
+    k_force_gather<float><<<(b.natoms + 255) / 256, 256, 0, s>>>(b, b.gselff, b.gentf);
+    k_struct_reduce<float><<<b.nstruct, kRedThreads, 0, s>>>(b, want_dEdLat, b.atEf, b.virf);
     return 2;
 }
 

@@ -1,0 +1,698 @@
+// symfn_fast.cu -- K4/K6 symmetry-function kernels on the potential's
+// lambda x zeta x eta grid ("product space"), FP64 or FP32.
+//
+// Same mathematics as symfn.cu (calcAllSymmetryFunctions,
+// symmetryFunctions.f90:158-308; scaling hdnnps.f90:471-481), organised so
+// that the per-(pair, SF) work is one fused multiply-add:
+//   * per pair: X_l = 1 + lambda_l cos, one square chain X, X^2, X^4, ...
+//     shared by every zeta, T_lz = X_l^zeta_z (and X_l^(zeta_z - 1) for the
+//     gradient), and one exponential Y_e = exp(-eta_e (r_ij^2+r_ik^2+r_jk^2))
+//     per distinct eta;
+//   * pass 1 accumulates acc[l,z,e] += T_lz Y_e fcp in registers and maps the
+//     product entries to SF indices at the end of each element-pair block
+//     (G_s = 2^(1-zeta) acc[l,z,e]);
+//   * pass 2 stages per block the weight tensors WA[l,z,e] = w_s 2^(1-zeta)
+//     and WC = WA lambda zeta (w_s = dE/dG_s / (max_s - min_s)) and contracts
+//     A = sum WA T Y, B = sum eta WA T Y, C = sum WC T' Y per pair, from which
+//     dE/dr_j and dE/dr_k are assembled as in symfn.cu.
+// Per-neighbour 1/r is precomputed, so a pair needs one sqrt, one tanh and
+// one exp per distinct eta.  Warp per centre atom; neighbours staged in
+// shared memory sorted by element; candidate pairs compacted through a shared
+// queue; chunks of 32 contributing pairs, one per lane.
+#include "engine.h"
+
+namespace hdnnp {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 4;
+
+template <typename T>
+struct alignas(4 * sizeof(T)) V4 {
+    T x, y, z, w;
+};
+
+__host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+
+template <typename T>
+struct FSmem {
+    V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
+    V4<double>* dd; // FP64 dx, dy, dz (FP32 form only; aliases nb in FP64)
+    V4<T>* ax;      // fc, dfc/r, 1/r, -
+    V4<T>* g;       // gradient accumulators (pass 2)
+    int* ent;       // entry index of a slot (pass 2)
+    unsigned char* el;
+    unsigned* queue;
+    int* est;
+    int* cur;
+    T* w;           // dE/dG / width (pass 2)
+    T* WA;          // [nblk][P] (pass 2)
+    T* WC;
+    T* red;         // [32][P+1] (pass 1)
+};
+
+template <typename T>
+__host__ __device__ inline size_t fast_warp_bytes(int mm, int nsf, int nblk, int P, bool grad) {
+    size_t b = a16(sizeof(V4<T>) * mm) * 2;
+    if (sizeof(T) == 4) b += a16(sizeof(V4<double>) * mm);
+    if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * nsf) + 2 * a16(sizeof(T) * nblk * P);
+    else b += a16(sizeof(T) * 32 * (P + 1));
+    b += a16(mm) + 64 * sizeof(unsigned) + a16(sizeof(int) * (kMaxEl + 1)) + a16(sizeof(int) * kMaxEl);
+    return b;
+}
+
+template <typename T>
+__device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int nsf, int nblk, int P, bool grad) {
+    FSmem<T> s{};
+    auto take = [&](size_t bytes) {
+        unsigned char* q = p;
+        p += a16(bytes);
+        return q;
+    };
+    s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
+    s.dd = sizeof(T) == 4 ? (V4<double>*)take(sizeof(V4<double>) * mm) : (V4<double>*)s.nb;
+    s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
+    if (grad) {
+        s.g = (V4<T>*)take(sizeof(V4<T>) * mm);
+        s.ent = (int*)take(sizeof(int) * mm);
+        s.w = (T*)take(sizeof(T) * nsf);
+        s.WA = (T*)take(sizeof(T) * nblk * P);
+        s.WC = (T*)take(sizeof(T) * nblk * P);
+    } else {
+        s.red = (T*)take(sizeof(T) * 32 * (P + 1));
+    }
+    s.el = (unsigned char*)take(mm);
+    s.queue = (unsigned*)take(64 * sizeof(unsigned));
+    s.est = (int*)take(sizeof(int) * (kMaxEl + 1));
+    s.cur = (int*)take(sizeof(int) * kMaxEl);
+    return s;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// precision-dispatched math
+__device__ __forceinline__ double xsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double xexp(double x) { return exp(x); }
+__device__ __forceinline__ float xexp(float x) { return expf(x); }
+__device__ __forceinline__ double xtanh(double x) { return tanh(x); }
+__device__ __forceinline__ float xtanh(float x) { return tanhf(x); }
+__device__ __forceinline__ double xpow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float xpow(float x, float y) { return powf(x, y); }
+
+template <typename T> struct Buf;
+template <> struct Buf<double> {
+    static __device__ double* G(const Batch& b) { return b.G; }
+    static __device__ const double* dEdG(const Batch& b) { return b.dEdG; }
+    static __device__ double* gent(const Batch& b) { return b.gent; }
+    static __device__ double* gself(const Batch& b) { return b.gself; }
+    static __device__ double* vir(const Batch& b) { return b.vir; }
+};
+template <> struct Buf<float> {
+    static __device__ float* G(const Batch& b) { return b.Gf; }
+    static __device__ const float* dEdG(const Batch& b) { return b.dEdGf; }
+    static __device__ float* gent(const Batch& b) { return b.gentf; }
+    static __device__ float* gself(const Batch& b) { return b.gselff; }
+    static __device__ float* vir(const Batch& b) { return b.virf; }
+};
+
+// Stage the neighbour entries of atom i sorted by element (stable).  The
+// relative vectors are formed in FP64 from the wrapped positions and image
+// shifts and then rounded to T.
+template <typename T, bool kGrad>
+__device__ void fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>& s, int lane, int M) {
+    const int e0 = b.nei_off[i];
+    const int nel = m.nel;
+    if (lane < nel) s.cur[lane] = 0;
+    __syncwarp();
+    for (int base = 0; base < M; base += 32) {
+        const int q = base + lane;
+        const unsigned act = __ballot_sync(kFull, q < M);
+        if (q < M) {
+            const int el = b.elem[b.nei_j[e0 + q]];
+            const unsigned peers = __match_any_sync(act, el);
+            if ((peers & lanemask_lt()) == 0) s.cur[el] += __popc(peers);
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        int acc = 0;
+        for (int x = 0; x < nel; ++x) {
+            s.est[x] = acc;
+            acc += s.cur[x];
+        }
+        s.est[nel] = acc;
+    }
+    __syncwarp();
+    if (lane < nel) s.cur[lane] = s.est[lane];
+    __syncwarp();
+    const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
+    const StructInfo& S = b.info[b.sid[i]];
+    const double rc = m.rc[c];
+    for (int base = 0; base < M; base += 32) {
+        const int q = base + lane;
+        const unsigned act = __ballot_sync(kFull, q < M);
+        int slot = 0, el = 0, j = 0, sh = 0;
+        if (q < M) {
+            j = b.nei_j[e0 + q];
+            sh = b.nei_s[e0 + q];
+            el = b.elem[j];
+            const unsigned peers = __match_any_sync(act, el);
+            slot = s.cur[el] + __popc(peers & lanemask_lt());
+            __syncwarp(act);
+            if ((peers & lanemask_lt()) == 0) s.cur[el] += __popc(peers);
+        }
+        __syncwarp();
+        if (q < M) {
+            int sx, sy, sz;
+            unpack_shift(sh, sx, sy, sz);
+            const double* h = S.h;
+            double lx = 0, ly = 0, lz = 0;
+            if (sz) { lx += h[6] * sz; ly += h[7] * sz; lz += h[8] * sz; }
+            if (sy) { lx += h[3] * sy; ly += h[4] * sy; lz += h[5] * sy; }
+            if (sx) { lx += h[0] * sx; ly += h[1] * sx; lz += h[2] * sx; }
+            const double dx = xi - (b.wpos[3 * j] + lx), dy = yi - (b.wpos[3 * j + 1] + ly),
+                         dz = zi - (b.wpos[3 * j + 2] + lz);
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            double fc = 0.0, dfc = 0.0;
+            if (r < rc) {
+                const double t = tanh(1.0 - r / rc), tt = t * t;
+                fc = tt * t;
+                dfc = -3.0 / (rc * r) * (tt - tt * tt);
+            }
+            s.nb[slot] = V4<T>{(T)dx, (T)dy, (T)dz, (T)r};
+            if (sizeof(T) == 4) s.dd[slot] = V4<double>{dx, dy, dz, r};
+            s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)(1.0 / r), (T)0};
+            s.el[slot] = (unsigned char)el;
+            if (kGrad) {
+                s.g[slot] = V4<T>{(T)0, (T)0, (T)0, (T)0};
+                s.ent[slot] = e0 + q;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Candidate c of block (a,b) -> slots (j,k) without divisions: rectangular
+// blocks use a float reciprocal of nb (exact for these sizes), triangular
+// blocks a float square root with integer fix-ups.
+__device__ __forceinline__ void fpair(int c, int sa, int na, int sb, int nb, bool same, float inv_nb, int& j, int& k) {
+    if (!same) {
+        int jj = (int)(((float)c + 0.5f) * inv_nb);
+        int kk = c - jj * nb;
+        if (kk < 0) { --jj; kk += nb; }
+        else if (kk >= nb) { ++jj; kk -= nb; }
+        j = sa + jj;
+        k = sb + kk;
+    } else {
+        const float t = (float)(2 * na - 1);
+        int jj = (int)((t - sqrtf(fmaxf(t * t - 8.0f * (float)c, 0.0f))) * 0.5f);
+        if (jj < 0) jj = 0;
+        auto off = [&](int x) { return x * (2 * na - x - 1) / 2; };
+        while (jj > 0 && off(jj) > c) --jj;
+        while (off(jj + 1) <= c) ++jj;
+        j = sa + jj;
+        k = sa + jj + 1 + (c - off(jj));
+    }
+}
+
+// u = 1 - r_jk/rc for the pair cutoff.  Near rc the difference cancels; it
+// is formed as (rc^2 - r_jk^2) / (rc (rc + r_jk)) with rc^2 - r_jk^2 taken
+// in FP64 from the FP64 relative vectors, so that the FP32 form keeps the
+// cutoff accurate to FP32 rounding even for pairs just inside rc (whose
+// SFs can have tiny scaling ranges and therefore large weights).
+template <typename T>
+__device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d, T rc, T rjk) {
+    const V4<double> a = s.dd[j], b = s.dd[k];
+    const double cx = b.x - a.x, cy = b.y - a.y, cz = b.z - a.z;
+    const double D = rc2d - (cx * cx + cy * cy + cz * cz);
+    return D > 0.0 ? (T)D / (rc * (rc + rjk)) : (T)0;
+}
+
+template <typename T>
+__device__ __forceinline__ void cutoff_pair(T u, T inv_r, T inv_rc, T& fc, T& dfc) {
+    if (u > (T)0) {
+        const T t = xtanh(u), tt = t * t;
+        fc = tt * t;
+        dfc = (T)(-3) * inv_rc * inv_r * (tt - tt * tt);
+    } else {
+        fc = (T)0;
+        dfc = (T)0;
+    }
+}
+
+// X^e for a model-wide (warp-uniform) integer e by the shared square chain.
+template <typename T>
+__device__ __forceinline__ T chain_pow(const T (&ch)[5], int e) {
+    T r = (T)1;
+#pragma unroll
+    for (int bit = 0; bit < 5; ++bit)
+        if ((e >> bit) & 1) r *= ch[bit];
+    return r;
+}
+
+// ---------------------------------------------------------------- pass 1
+template <typename T, int NL, int NZ, int NE>
+__global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, int mm) {
+    constexpr int P = NL * NZ * NE;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, false), mm, m.nsf_max,
+                           m.nblk, P, false);
+    const int nel = m.nel;
+    T* Gout = Buf<T>::G(b);
+    for (int i = blockIdx.x * kWarps + wib; i < b.natoms; i += gridDim.x * kWarps) {
+        const int c = b.elem[i];
+        if (c < 0) continue;
+        const int M = b.nei_off[i + 1] - b.nei_off[i];
+        if (M > mm) {
+            if (lane == 0) atomicOr(&b.status[0], 4);
+            continue;
+        }
+        fstage<T, false>(b, m, i, c, s, lane, M);
+        const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
+        const double rc2d = m.rc[c] * m.rc[c];
+        T* Gi = Gout + (size_t)i * m.nsf_max;
+        const double* mean = m.smean + (size_t)c * m.nsf_max;
+        const double* width = m.swidth + (size_t)c * m.nsf_max;
+
+        // radial SFs: lane = SF
+        const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
+        for (int f = r0 + lane; f < r1; f += 32) {
+            const SF2 q = m.g2[f];
+            const T eta = (T)q.eta, rs = (T)q.rs;
+            T acc = (T)0;
+            for (int t = s.est[q.nel]; t < s.est[q.nel + 1]; ++t) {
+                const T x = s.nb[t].w - rs;
+                acc += xexp(-eta * x * x) * s.ax[t].x;
+            }
+            Gi[q.sf] = (T)(((double)acc - mean[q.sf]) / width[q.sf]);
+        }
+
+        unsigned long long n_cand = 0, n_pairs = 0;
+        for (int t = 0; t < m.nblk; ++t) {
+            const int gb = m.g4_off[c * m.nblk + t], ge = m.g4_off[c * m.nblk + t + 1];
+            if (ge == gb) continue;
+            const int ea = m.blk_a[t], eb = m.blk_b[t];
+            const int sa = s.est[ea], na = s.est[ea + 1] - sa;
+            const int sb = s.est[eb], nb = s.est[eb + 1] - sb;
+            const bool same = (ea == eb);
+            const int ncand = same ? na * (na - 1) / 2 : na * nb;
+            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+            n_cand += ncand;
+            T acc[P];
+#pragma unroll
+            for (int p = 0; p < P; ++p) acc[p] = (T)0;
+            int qlen = 0;
+            for (int cb = 0; cb < ncand; cb += 32) {
+                const int cidx = cb + lane;
+                bool ok = cidx < ncand;
+                int j = 0, k = 0;
+                if (ok) {
+                    fpair(cidx, sa, na, sb, nb, same, inv_nb, j, k);
+                    const V4<T> a = s.nb[j], bb = s.nb[k];
+                    const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
+                    ok = ex * ex + ey * ey + ez * ez < rc2;
+                }
+                const unsigned bal = __ballot_sync(kFull, ok);
+                if (ok) s.queue[qlen + __popc(bal & lanemask_lt())] = (unsigned)j | ((unsigned)k << 16);
+                qlen += __popc(bal);
+                n_pairs += __popc(bal);
+                __syncwarp();
+                const bool last = cb + 32 >= ncand;
+                while (qlen >= 32 || (last && qlen > 0)) {
+                    const int n = qlen < 32 ? qlen : 32;
+                    if (lane < n) {
+                        const unsigned pk = s.queue[lane];
+                        const int pj = pk & 0xffff, pq = pk >> 16;
+                        const V4<T> a = s.nb[pj], bq = s.nb[pq];
+                        const V4<T> xa = s.ax[pj], xb = s.ax[pq];
+                        const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;
+                        const T rjk2 = cx * cx + cy * cy + cz * cz;
+                        const T rjk = xsqrt(rjk2);
+                        const T u = pair_u(s, pj, pq, rc2d, rc, rjk);
+                        T fjk = (T)0;
+                        if (u > (T)0) {
+                            const T tj = xtanh(u);
+                            fjk = tj * tj * tj;
+                        }
+                        const T t1 = -xa.z * xb.z;  // -1/(rj rk)
+                        const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
+                        const T fcp = xa.x * xb.x * fjk;
+                        const T R = a.w * a.w + bq.w * bq.w + rjk2;
+                        T Y[NE];
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) Y[e] = e < m.fe ? xexp(-(T)m.eta4[e] * R) * fcp : (T)0;
+#pragma unroll
+                        for (int l = 0; l < NL; ++l) {
+                            const T X = (T)1 + (T)m.lam[l] * cth;
+                            T ch[5];
+                            ch[0] = X;
+#pragma unroll
+                            for (int bit = 1; bit < 5; ++bit) ch[bit] = bit <= m.zmaxbit ? ch[bit - 1] * ch[bit - 1] : (T)0;
+#pragma unroll
+                            for (int z = 0; z < NZ; ++z) {
+                                T Tz = (T)0;
+                                if (z < m.fz) {
+                                    const int ez = m.zint[z];
+                                    Tz = ez >= 0 ? chain_pow(ch, ez + 1) : xpow(X, (T)m.zet[z]);
+                                }
+#pragma unroll
+                                for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz * Y[e];
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    const int rem = qlen - n;
+                    unsigned v = 0;
+                    if (lane < rem) v = s.queue[n + lane];
+                    __syncwarp();
+                    if (lane < rem) s.queue[lane] = v;
+                    __syncwarp();
+                    qlen = rem;
+                }
+            }
+            // warp reduction of acc[P] through shared memory (row stride P+1)
+#pragma unroll
+            for (int p = 0; p < P; ++p) s.red[lane * (P + 1) + p] = acc[p];
+            __syncwarp();
+            constexpr int NH = 32 / P > 0 ? 32 / P : 1;
+            const int p = lane % P, h = lane / P;
+            T sum = (T)0;
+            if (h < NH)
+                for (int r = h; r < 32; r += NH) sum += s.red[r * (P + 1) + p];
+#pragma unroll
+            for (int off = P; off < 32; off <<= 1) sum += __shfl_xor_sync(kFull, sum, off);
+            __syncwarp();
+            if (lane < P) {
+                const int sf = m.pmap[((size_t)c * m.nblk + t) * P + lane];
+                if (sf >= 0) {
+                    const int z = (lane / NE) % NZ;
+                    Gi[sf] = (T)(((double)((T)m.pfz[z] * sum) - mean[sf]) / width[sf]);
+                }
+            }
+        }
+        if (b.stats && lane == 0) {
+            unsigned long long n2 = 0, n4 = 0;
+            for (int f = r0; f < r1; ++f) n2 += s.est[m.g2[f].nel + 1] - s.est[m.g2[f].nel];
+            (void)n4;
+            atomicAdd(&b.stats[2], (unsigned long long)M);
+            atomicAdd(&b.stats[3], n_cand);
+            atomicAdd(&b.stats[6], n2);
+        }
+        if (b.stats) {
+            // pairs and G4 terms: one lane adds the warp total
+            unsigned long long tot = n_pairs;  // identical on every lane (from ballots)
+            if (lane == 0) {
+                atomicAdd(&b.stats[4], tot);
+                unsigned long long terms = 0;
+                (void)terms;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- pass 2
+template <typename T, int NL, int NZ, int NE>
+__global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, int mm) {
+    constexpr int P = NL * NZ * NE;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, true), mm, m.nsf_max,
+                           m.nblk, P, true);
+    const int nel = m.nel;
+    const T* dEdG = Buf<T>::dEdG(b);
+    for (int i = blockIdx.x * kWarps + wib; i < b.natoms; i += gridDim.x * kWarps) {
+        const int c = b.elem[i];
+        if (c < 0) continue;
+        const int M = b.nei_off[i + 1] - b.nei_off[i];
+        if (M > mm) {
+            if (lane == 0) atomicOr(&b.status[0], 4);
+            continue;
+        }
+        fstage<T, true>(b, m, i, c, s, lane, M);
+        const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
+        const double rc2d = m.rc[c] * m.rc[c];
+        const int nsf = m.nsf[c];
+        for (int q = lane; q < nsf; q += 32)
+            s.w[q] = (T)((double)dEdG[(size_t)i * m.nsf_max + q] / m.swidth[(size_t)c * m.nsf_max + q]);
+        __syncwarp();
+        for (int q = lane; q < m.nblk * P; q += 32) {
+            const int t = q / P, p = q % P;
+            const int sf = m.pmap[((size_t)c * m.nblk + t) * P + p];
+            T wa = (T)0, wc = (T)0;
+            if (sf >= 0) {
+                const int l = p / (NZ * NE), z = (p / NE) % NZ;
+                wa = s.w[sf] * (T)m.pfz[z];
+                wc = wa * (T)m.lam[l] * (T)m.zet[z];
+            }
+            s.WA[q] = wa;
+            s.WC[q] = wc;
+        }
+        __syncwarp();
+
+        // radial: lane = neighbour slot
+        for (int t = lane; t < M; t += 32) {
+            const int el = s.el[t];
+            const int f0 = m.g2_off[c * nel + el], f1 = m.g2_off[c * nel + el + 1];
+            const V4<T> d = s.nb[t];
+            const V4<T> x = s.ax[t];
+            T coef = (T)0;
+            for (int f = f0; f < f1; ++f) {
+                const SF2 q = m.g2[f];
+                const T eta = (T)q.eta, xr = d.w - (T)q.rs;
+                const T e = xexp(-eta * xr * xr);
+                coef += s.w[q.sf] * (-e * x.y + (T)2 * eta * xr * x.z * e * x.x);
+            }
+            V4<T> g = s.g[t];
+            g.x += coef * d.x;
+            g.y += coef * d.y;
+            g.z += coef * d.z;
+            s.g[t] = g;
+        }
+        __syncwarp();
+
+        // angular: the queue spans element-pair blocks (entries carry the block)
+        int qlen = 0;
+        for (int t = 0; t < m.nblk; ++t) {
+            const int gb = m.g4_off[c * m.nblk + t], ge = m.g4_off[c * m.nblk + t + 1];
+            const bool has = ge > gb;
+            const int ea = m.blk_a[t], eb = m.blk_b[t];
+            const int sa = s.est[ea], na = s.est[ea + 1] - sa;
+            const int sb = s.est[eb], nb = s.est[eb + 1] - sb;
+            const bool same = (ea == eb);
+            const int ncand = has ? (same ? na * (na - 1) / 2 : na * nb) : 0;
+            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+            const bool last_blk = (t == m.nblk - 1);
+            for (int cb = 0; cb < ncand || (last_blk && cb == 0); cb += 32) {
+                const int cidx = cb + lane;
+                bool ok = cidx < ncand;
+                int j = 0, k = 0;
+                if (ok) {
+                    fpair(cidx, sa, na, sb, nb, same, inv_nb, j, k);
+                    const V4<T> a = s.nb[j], bb = s.nb[k];
+                    const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
+                    ok = ex * ex + ey * ey + ez * ez < rc2;
+                }
+                const unsigned bal = __ballot_sync(kFull, ok);
+                if (ok) s.queue[qlen + __popc(bal & lanemask_lt())] = (unsigned)j | ((unsigned)k << 10) | ((unsigned)t << 20);
+                qlen += __popc(bal);
+                __syncwarp();
+                const bool flush_all = last_blk && cb + 32 >= ncand;
+                while (qlen >= 32 || (flush_all && qlen > 0)) {
+                    const int n = qlen < 32 ? qlen : 32;
+                    if (lane < n) {
+                        const unsigned pk = s.queue[lane];
+                        const int pj = pk & 0x3ff, pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
+                        const V4<T> a = s.nb[pj], bq = s.nb[pq];
+                        const V4<T> xa = s.ax[pj], xb = s.ax[pq];
+                        const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
+                        const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;  // djk = r_j - r_k
+                        const T rjk2 = cx * cx + cy * cy + cz * cz;
+                        const T rjk = xsqrt(rjk2);
+                        T fjk, dfjk;
+                        cutoff_pair(pair_u(s, pj, pq, rc2d, rc, rjk), (T)1 / rjk, inv_rc, fjk, dfjk);
+                        const T irj = xa.z, irk = xb.z;
+                        const T t1 = -irj * irk;
+                        const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
+                        const T dot = a.x * bq.x + a.y * bq.y + a.z * bq.z;
+                        const T cj = dot * irj * irj * irj * irk, ck = dot * irk * irk * irk * irj;
+                        const T fcp = fj * fk * fjk;
+                        const T R = a.w * a.w + bq.w * bq.w + rjk2;
+                        T Y[NE];
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) Y[e] = e < m.fe ? xexp(-(T)m.eta4[e] * R) : (T)0;
+                        T SA[NE], SC[NE];
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
+                        const T* wa = s.WA + pt * P;
+                        const T* wc = s.WC + pt * P;
+#pragma unroll
+                        for (int l = 0; l < NL; ++l) {
+                            const T X = (T)1 + (T)m.lam[l] * cth;
+                            T ch[5];
+                            ch[0] = X;
+#pragma unroll
+                            for (int bit = 1; bit < 5; ++bit) ch[bit] = bit <= m.zmaxbit ? ch[bit - 1] * ch[bit - 1] : (T)0;
+#pragma unroll
+                            for (int z = 0; z < NZ; ++z) {
+                                T Tp = (T)0, Tz = (T)0;
+                                if (z < m.fz) {
+                                    const int ez = m.zint[z];
+                                    Tp = ez >= 0 ? chain_pow(ch, ez) : xpow(X, (T)m.zet[z] - (T)1);
+                                    Tz = Tp * X;
+                                }
+#pragma unroll
+                                for (int e = 0; e < NE; ++e) {
+                                    SA[e] += wa[(l * NZ + z) * NE + e] * Tz;
+                                    SC[e] += wc[(l * NZ + z) * NE + e] * Tp;
+                                }
+                            }
+                        }
+                        T A = (T)0, B = (T)0, C = (T)0;
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) {
+                            A += Y[e] * SA[e];
+                            B += (T)m.eta4[e] * Y[e] * SA[e];
+                            C += Y[e] * SC[e];
+                        }
+                        const T B2 = (T)2 * B * fcp, Cf = C * fcp;
+                        const T pj1 = A * fk * fj * dfjk, pj2 = A * fk * dfj * fjk;
+                        const T pk1 = A * fj * fk * dfjk, pk2 = A * fj * dfk * fjk;
+                        const T gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
+                        const T gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
+                        const T gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
+                        const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
+                        const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
+                        const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
+                        atomicAdd(&s.g[pj].x, gjx);
+                        atomicAdd(&s.g[pj].y, gjy);
+                        atomicAdd(&s.g[pj].z, gjz);
+                        atomicAdd(&s.g[pq].x, gkx);
+                        atomicAdd(&s.g[pq].y, gky);
+                        atomicAdd(&s.g[pq].z, gkz);
+                    }
+                    __syncwarp();
+                    const int rem = qlen - n;
+                    unsigned v = 0;
+                    if (lane < rem) v = s.queue[n + lane];
+                    __syncwarp();
+                    if (lane < rem) s.queue[lane] = v;
+                    __syncwarp();
+                    qlen = rem;
+                }
+            }
+        }
+        __syncwarp();
+        T* gent = Buf<T>::gent(b);
+        T sx = 0, sy = 0, sz = 0;
+        T v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int t = lane; t < M; t += 32) {
+            const V4<T> g = s.g[t];
+            const V4<T> d = s.nb[t];
+            const size_t e = (size_t)s.ent[t];
+            gent[3 * e] = g.x;
+            gent[3 * e + 1] = g.y;
+            gent[3 * e + 2] = g.z;
+            sx -= g.x;
+            sy -= g.y;
+            sz -= g.z;
+            v[0] -= g.x * d.x; v[1] -= g.y * d.x; v[2] -= g.z * d.x;
+            v[3] -= g.x * d.y; v[4] -= g.y * d.y; v[5] -= g.z * d.y;
+            v[6] -= g.x * d.z; v[7] -= g.y * d.z; v[8] -= g.z * d.z;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(kFull, sx, o);
+            sy += __shfl_xor_sync(kFull, sy, o);
+            sz += __shfl_xor_sync(kFull, sz, o);
+#pragma unroll
+            for (int u = 0; u < 9; ++u) v[u] += __shfl_xor_sync(kFull, v[u], o);
+        }
+        if (lane == 0) {
+            T* gs = Buf<T>::gself(b);
+            T* vr = Buf<T>::vir(b);
+            gs[3 * (size_t)i] = sx;
+            gs[3 * (size_t)i + 1] = sy;
+            gs[3 * (size_t)i + 2] = sz;
+#pragma unroll
+            for (int u = 0; u < 9; ++u) vr[9 * (size_t)i + u] = v[u];
+        }
+        __syncwarp();
+    }
+}
+
+int nsm() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <typename K>
+void set_smem(K kernel, size_t smem) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename T, int NL, int NZ, int NE>
+void run_shape(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
+    constexpr int P = NL * NZ * NE;
+    const int mm = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
+    const size_t smem = fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, grad) * kWarps;
+    int blocks = (b.natoms + kWarps - 1) / kWarps;
+    const int cap = nsm() * 32;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    if (grad) {
+        set_smem(k_sfg_fast<T, NL, NZ, NE>, smem);
+        k_sfg_fast<T, NL, NZ, NE><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+    } else {
+        set_smem(k_sfv_fast<T, NL, NZ, NE>, smem);
+        k_sfv_fast<T, NL, NZ, NE><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+    }
+}
+
+template <typename T>
+void run_any(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
+    switch (m.fast) {
+        case 1: run_shape<T, 2, 2, 1>(b, m, grad, st); break;
+        case 2: run_shape<T, 2, 4, 2>(b, m, grad, st); break;
+        case 3: run_shape<T, 2, 4, 4>(b, m, grad, st); break;
+        case 4: run_shape<T, 2, 8, 2>(b, m, grad, st); break;
+        default: break;
+    }
+}
+
+}  // namespace
+
+size_t sf_fast_smem_per_warp(int mmax, int nsf, int nblk, int P, bool grad, bool fp32) {
+    const int mm = mmax > 0 ? ((mmax + 31) / 32) * 32 : 32;
+    return fp32 ? fast_warp_bytes<float>(mm, nsf, nblk, P, grad) : fast_warp_bytes<double>(mm, nsf, nblk, P, grad);
+}
+
+int launch_sf_values_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t st) {
+    if (fp32)
+        run_any<float>(b, m, false, st);
+    else
+        run_any<double>(b, m, false, st);
+    return 1;
+}
+
+int launch_sf_gradients_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t st) {
+    if (fp32)
+        run_any<float>(b, m, true, st);
+    else
+        run_any<double>(b, m, true, st);
+    return 1;
+}
+
+}  // namespace hdnnp

@@ -64,6 +64,7 @@ def lib():
     L.hdnnp_ctx_free.argtypes = [P]
     L.hdnnp_ctx_free.restype = None
     L.hdnnp_ctx_set_precision.argtypes = [P, C.c_int]
+    L.hdnnp_ctx_set_option.argtypes = [P, C.c_char_p, C.c_int]
     L.hdnnp_energy_and_forces.argtypes = [P, C.c_int, I, D, C.c_int, D, D, D, D]
     L.hdnnp_eval_batch.argtypes = [P, C.c_int, I64, I, D, I, D, D, D, D]
     L.hdnnp_eval_batch_device.argtypes = [P, C.c_int, I64, P, P, P, I, D, P, P, P, P]
@@ -155,6 +156,9 @@ class Hdnnp:
             self.close()
         except Exception:
             pass
+
+    def set_option(self, name: str, value: int):
+        _check(lib().hdnnp_ctx_set_option(self._c, name.encode(), int(value)))
 
     def set_precision(self, mode: int):
         _check(lib().hdnnp_ctx_set_precision(self._c, int(mode)))

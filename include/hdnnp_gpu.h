@@ -77,6 +77,11 @@ int hdnnp_ctx_create(hdnnp_model* m, hdnnp_ctx** out);
 void hdnnp_ctx_free(hdnnp_ctx* c);
 int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
 
+/* Context options (for tests and tuning): "generic_sf" = 1 forces the
+ * generic symmetry-function kernels (one parameter record per SF) instead of
+ * the lambda x zeta x eta kernels; the result is the same within rounding.   */
+int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
+
 /* ---------------------------------------------------------------- evaluation
  * Replaces hdnnpEnergyAndForces(handle, ats, energy, force, dEdLat)
  * (hdnnps.f90:333-371): neighbour lists (hdnnpCalcNeighborLists :373),

@@ -141,3 +141,16 @@ def test_errors_are_status_codes(eng, gab, W):
     # the context stays usable after errors
     E, F, _ = gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], c["lat"]))
     assert np.isfinite(E)
+
+
+def test_generic_and_fast_kernels_agree(eng, gab, abx3_model, W):
+    s = W.config_c4(n_struct=6, seed=13)
+    fast = gab.eval_batch(s, dEdLat=True)
+    gab.set_option("generic_sf", 1)
+    try:
+        gen = gab.eval_batch(s, dEdLat=True)
+    finally:
+        gab.set_option("generic_sf", 0)
+    assert np.abs(fast["energy"] - gen["energy"]).max() <= E_REL * np.abs(gen["energy"]).max()
+    assert np.abs(fast["forces"] - gen["forces"]).max() <= F_ABS
+    assert np.abs(fast["dEdLat"] - gen["dEdLat"]).max() <= L_ABS
