@@ -174,6 +174,7 @@ struct hdnnp_ctx {
     cudaStream_t stream = nullptr;
     int precision = HDNNP_PREC_FP64;
     int generic_sf = 0;
+    int runtime_zeta = 0;
     int launches = 0;
     // device buffers
     DevBuf<StructInfo> info;
@@ -307,7 +308,14 @@ int upload_model(hdnnp_model* m) {
             if (std::fabs(z - iz) < 1e-10 && iz >= 1) maxz = std::max(maxz, iz);
             if (z > 31.0) ints_ok = false;
         }
-        for (int id = 1; id <= 4 && ints_ok; ++id)
+        // a compiled zeta set that matches exactly (same count of zeta and eta)
+        for (int id = 5; id < kNumFastShapes && ints_ok && !shape; ++id) {
+            bool match = (int)lams.size() <= kFastShapes[id][0] && (int)zets.size() == kFastShapes[id][1] &&
+                         (int)etas.size() == kFastShapes[id][2];
+            for (size_t z = 0; match && z < zets.size(); ++z) match = zets[z] == (double)kFastZeta[id][z];
+            if (match) shape = id;
+        }
+        for (int id = 1; id <= 4 && ints_ok && !shape; ++id)
             if ((int)lams.size() <= kFastShapes[id][0] && (int)zets.size() <= kFastShapes[id][1] &&
                 (int)etas.size() <= kFastShapes[id][2]) {
                 shape = id;
@@ -452,7 +460,10 @@ int collect_profile(hdnnp_ctx* c) {
 int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const double* posd, double* energy_d,
                  double* force_d, double* dEdLat_d, cudaStream_t st) {
     hdnnp_model* m = c->model;
-    const DevModel& D = m->dev;
+    DevModel D = m->dev;
+    // runtime-zeta variant of a compiled-zeta shape (same product layout)
+    if (c->runtime_zeta && D.fast == 5) D.fast = 1;
+    if (c->runtime_zeta && D.fast == 6) D.fast = 2;
     int ncells = 0;
     for (auto& S : c->hinfo) {
         S.cell_off = ncells;
@@ -689,6 +700,10 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
     if (!c || !name) return fail(HDNNP_E_INPUT, "null argument");
     if (std::string(name) == "generic_sf") {
         c->generic_sf = value != 0;
+        return HDNNP_OK;
+    }
+    if (std::string(name) == "runtime_zeta") {
+        c->runtime_zeta = value != 0;
         return HDNNP_OK;
     }
     return fail(HDNNP_E_INPUT, std::string("unknown option ") + name);

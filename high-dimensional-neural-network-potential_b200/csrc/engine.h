@@ -171,7 +171,12 @@ size_t mlp_smem_bytes(const DevModel& m, size_t elem);
 size_t sf_smem_per_warp(int mmax, bool grad);
 
 // Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).
-constexpr int kFastShapes[5][3] = {{0, 0, 0}, {2, 2, 1}, {2, 4, 2}, {2, 4, 4}, {2, 8, 2}};
+// Ids 1-4 read zeta from the model; ids 5-6 have the zeta set compiled in
+// (kFastZeta) and are preferred when the potential's zeta set matches.
+constexpr int kNumFastShapes = 7;
+constexpr int kFastShapes[kNumFastShapes][3] = {{0, 0, 0}, {2, 2, 1}, {2, 4, 2}, {2, 4, 4},
+                                                {2, 8, 2}, {2, 2, 1}, {2, 4, 2}};
+constexpr int kFastZeta[kNumFastShapes][4] = {{0}, {0}, {0}, {0}, {0}, {1, 4, 0, 0}, {1, 2, 4, 16}};
 inline int fast_shape_p(int id) { return kFastShapes[id][0] * kFastShapes[id][1] * kFastShapes[id][2]; }
 
 // Fast (product-space) symmetry-function kernels, FP64 (T = double) or FP32.

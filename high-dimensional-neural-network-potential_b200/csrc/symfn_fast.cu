@@ -234,21 +234,38 @@ __device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d
     return D > 0.0 ? (T)D / (rc * (rc + rjk)) : (T)0;
 }
 
-template <typename T>
-__device__ __forceinline__ void cutoff_pair(T u, T inv_r, T inv_rc, T& fc, T& dfc) {
-    if (u > (T)0) {
-        const T t = xtanh(u), tt = t * t;
-        fc = tt * t;
-        dfc = (T)(-3) * inv_rc * inv_r * (tt - tt * tt);
-    } else {
-        fc = (T)0;
-        dfc = (T)0;
+// ---------------------------------------------------------------- grid specs
+// Spec<NL, NZ, NE, Z0..Z3>: compiled shape of the lambda x zeta x eta grid.
+// With Z0 > 0 the zeta values are compile-time constants (the power chain and
+// every product are straight-line code); with Z0 == 0 they are read from the
+// model (uniform branches).
+template <int NL_, int NZ_, int NE_, int Z0 = 0, int Z1 = 0, int Z2 = 0, int Z3 = 0>
+struct Spec {
+    static constexpr int NL = NL_, NZ = NZ_, NE = NE_, P = NL_ * NZ_ * NE_;
+    static constexpr bool kFixed = Z0 > 0;
+    __host__ __device__ static constexpr int zeta(int z) { return z == 0 ? Z0 : z == 1 ? Z1 : z == 2 ? Z2 : Z3; }
+    __host__ __device__ static constexpr int maxbit() {
+        int mz = 1;
+        for (int z = 0; z < NZ_; ++z) mz = zeta(z) > mz ? zeta(z) : mz;
+        int b = 0;
+        while ((1 << (b + 1)) <= mz) ++b;
+        return b;
     }
+};
+
+// X^E from the square chain ch[b] = X^(2^b); E is a compile-time constant
+// after unrolling, so the bit tests fold away.
+template <int E, typename T>
+__device__ __forceinline__ T cpow(const T (&ch)[5]) {
+    T r = (T)1;
+#pragma unroll
+    for (int bit = 0; bit < 5; ++bit)
+        if ((E >> bit) & 1) r = r * ch[bit];
+    return r;
 }
 
-// X^e for a model-wide (warp-uniform) integer e by the shared square chain.
 template <typename T>
-__device__ __forceinline__ T chain_pow(const T (&ch)[5], int e) {
+__device__ __forceinline__ T rpow(const T (&ch)[5], int e) {
     T r = (T)1;
 #pragma unroll
     for (int bit = 0; bit < 5; ++bit)
@@ -256,16 +273,70 @@ __device__ __forceinline__ T chain_pow(const T (&ch)[5], int e) {
     return r;
 }
 
+// Tz[z] = X^zeta_z and (kDeriv) Tp[z] = X^(zeta_z - 1) for one lambda.
+template <class S, bool kDeriv, typename T>
+__device__ __forceinline__ void powers(const DevModel& m, T X, T (&Tz)[S::NZ], T (&Tp)[S::NZ]) {
+    T ch[5];
+    ch[0] = X;
+    if constexpr (S::kFixed) {
+        constexpr int mb = S::maxbit();
+#pragma unroll
+        for (int b = 1; b < 5; ++b) ch[b] = b <= mb ? ch[b - 1] * ch[b - 1] : (T)0;
+#pragma unroll
+        for (int z = 0; z < S::NZ; ++z) {
+            if constexpr (kDeriv) {
+                // X^(zeta-1) from the chain, X^zeta = X^(zeta-1) * X
+                T p = (T)1;
+#pragma unroll
+                for (int bit = 0; bit < 5; ++bit)
+                    if (((S::zeta(z) - 1) >> bit) & 1) p = p * ch[bit];
+                Tp[z] = p;
+                Tz[z] = p * X;
+            } else {
+                T p = (T)1;
+#pragma unroll
+                for (int bit = 0; bit < 5; ++bit)
+                    if ((S::zeta(z) >> bit) & 1) p = p * ch[bit];
+                Tz[z] = p;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int b = 1; b < 5; ++b) ch[b] = b <= m.zmaxbit ? ch[b - 1] * ch[b - 1] : (T)0;
+#pragma unroll
+        for (int z = 0; z < S::NZ; ++z) {
+            T p = (T)0, q = (T)0;
+            if (z < m.fz) {
+                const int ez = m.zint[z];
+                if (kDeriv) {
+                    p = ez >= 0 ? rpow(ch, ez) : xpow(X, (T)m.zet[z] - (T)1);
+                    q = p * X;
+                } else {
+                    q = ez >= 0 ? rpow(ch, ez + 1) : xpow(X, (T)m.zet[z]);
+                }
+            }
+            Tz[z] = q;
+            if (kDeriv) Tp[z] = p;
+        }
+    }
+}
+
+template <class S>
+__device__ __forceinline__ int n_eta(const DevModel& m) {
+    return S::kFixed ? S::NE : m.fe;
+}
+
 // ---------------------------------------------------------------- pass 1
-template <typename T, int NL, int NZ, int NE>
+template <typename T, class S>
 __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, int mm) {
-    constexpr int P = NL * NZ * NE;
+    constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, false), mm, m.nsf_max,
                            m.nblk, P, false);
     const int nel = m.nel;
     T* Gout = Buf<T>::G(b);
+    const int ne = n_eta<S>(m);
     for (int i = blockIdx.x * kWarps + wib; i < b.natoms; i += gridDim.x * kWarps) {
         const int c = b.elem[i];
         if (c < 0) continue;
@@ -335,36 +406,23 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
                         const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;
                         const T rjk2 = cx * cx + cy * cy + cz * cz;
                         const T rjk = xsqrt(rjk2);
-                        const T u = pair_u(s, pj, pq, rc2d, rc, rjk);
-                        T fjk = (T)0;
-                        if (u > (T)0) {
-                            const T tj = xtanh(u);
-                            fjk = tj * tj * tj;
-                        }
+                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk));
+                        const T fjk = tj * tj * tj;
                         const T t1 = -xa.z * xb.z;  // -1/(rj rk)
                         const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
                         const T fcp = xa.x * xb.x * fjk;
                         const T R = a.w * a.w + bq.w * bq.w + rjk2;
                         T Y[NE];
 #pragma unroll
-                        for (int e = 0; e < NE; ++e) Y[e] = e < m.fe ? xexp(-(T)m.eta4[e] * R) * fcp : (T)0;
+                        for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) * fcp : (T)0;
 #pragma unroll
                         for (int l = 0; l < NL; ++l) {
-                            const T X = (T)1 + (T)m.lam[l] * cth;
-                            T ch[5];
-                            ch[0] = X;
+                            T Tz[NZ], Tp[NZ];
+                            powers<S, false>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
 #pragma unroll
-                            for (int bit = 1; bit < 5; ++bit) ch[bit] = bit <= m.zmaxbit ? ch[bit - 1] * ch[bit - 1] : (T)0;
+                            for (int z = 0; z < NZ; ++z)
 #pragma unroll
-                            for (int z = 0; z < NZ; ++z) {
-                                T Tz = (T)0;
-                                if (z < m.fz) {
-                                    const int ez = m.zint[z];
-                                    Tz = ez >= 0 ? chain_pow(ch, ez + 1) : xpow(X, (T)m.zet[z]);
-                                }
-#pragma unroll
-                                for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz * Y[e];
-                            }
+                                for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz[z] * Y[e];
                         }
                     }
                     __syncwarp();
@@ -378,14 +436,18 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
                 }
             }
             // warp reduction of acc[P] through shared memory (row stride P+1)
+            {
+                T* row = s.red + lane * (P + 1);
 #pragma unroll
-            for (int p = 0; p < P; ++p) s.red[lane * (P + 1) + p] = acc[p];
+                for (int p = 0; p < P; ++p) row[p] = acc[p];
+            }
             __syncwarp();
             constexpr int NH = 32 / P > 0 ? 32 / P : 1;
             const int p = lane % P, h = lane / P;
             T sum = (T)0;
             if (h < NH)
-                for (int r = h; r < 32; r += NH) sum += s.red[r * (P + 1) + p];
+#pragma unroll
+                for (int r = 0; r < 32 / NH; ++r) sum += s.red[(h + r * NH) * (P + 1) + p];
 #pragma unroll
             for (int off = P; off < 32; off <<= 1) sum += __shfl_xor_sync(kFull, sum, off);
             __syncwarp();
@@ -398,36 +460,29 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
             }
         }
         if (b.stats && lane == 0) {
-            unsigned long long n2 = 0, n4 = 0;
+            unsigned long long n2 = 0;
             for (int f = r0; f < r1; ++f) n2 += s.est[m.g2[f].nel + 1] - s.est[m.g2[f].nel];
-            (void)n4;
             atomicAdd(&b.stats[2], (unsigned long long)M);
             atomicAdd(&b.stats[3], n_cand);
+            atomicAdd(&b.stats[4], n_pairs);
+            atomicAdd(&b.stats[5], n_pairs * (unsigned long long)P);
             atomicAdd(&b.stats[6], n2);
-        }
-        if (b.stats) {
-            // pairs and G4 terms: one lane adds the warp total
-            unsigned long long tot = n_pairs;  // identical on every lane (from ballots)
-            if (lane == 0) {
-                atomicAdd(&b.stats[4], tot);
-                unsigned long long terms = 0;
-                (void)terms;
-            }
         }
         __syncwarp();
     }
 }
 
 // ---------------------------------------------------------------- pass 2
-template <typename T, int NL, int NZ, int NE>
+template <typename T, class S>
 __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, int mm) {
-    constexpr int P = NL * NZ * NE;
+    constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, true), mm, m.nsf_max,
                            m.nblk, P, true);
     const int nel = m.nel;
     const T* dEdG = Buf<T>::dEdG(b);
+    const int ne = n_eta<S>(m);
     for (int i = blockIdx.x * kWarps + wib; i < b.natoms; i += gridDim.x * kWarps) {
         const int c = b.elem[i];
         if (c < 0) continue;
@@ -516,8 +571,10 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                         const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;  // djk = r_j - r_k
                         const T rjk2 = cx * cx + cy * cy + cz * cz;
                         const T rjk = xsqrt(rjk2);
-                        T fjk, dfjk;
-                        cutoff_pair(pair_u(s, pj, pq, rc2d, rc, rjk), (T)1 / rjk, inv_rc, fjk, dfjk);
+                        const T irjk = (T)1 / rjk;
+                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk)), tt = tj * tj;
+                        const T fjk = tt * tj;
+                        const T dfjk = (T)(-3) * inv_rc * irjk * (tt - tt * tt);
                         const T irj = xa.z, irk = xb.z;
                         const T t1 = -irj * irk;
                         const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
@@ -527,7 +584,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                         const T R = a.w * a.w + bq.w * bq.w + rjk2;
                         T Y[NE];
 #pragma unroll
-                        for (int e = 0; e < NE; ++e) Y[e] = e < m.fe ? xexp(-(T)m.eta4[e] * R) : (T)0;
+                        for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) : (T)0;
                         T SA[NE], SC[NE];
 #pragma unroll
                         for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
@@ -535,25 +592,15 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                         const T* wc = s.WC + pt * P;
 #pragma unroll
                         for (int l = 0; l < NL; ++l) {
-                            const T X = (T)1 + (T)m.lam[l] * cth;
-                            T ch[5];
-                            ch[0] = X;
+                            T Tz[NZ], Tp[NZ];
+                            powers<S, true>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
 #pragma unroll
-                            for (int bit = 1; bit < 5; ++bit) ch[bit] = bit <= m.zmaxbit ? ch[bit - 1] * ch[bit - 1] : (T)0;
-#pragma unroll
-                            for (int z = 0; z < NZ; ++z) {
-                                T Tp = (T)0, Tz = (T)0;
-                                if (z < m.fz) {
-                                    const int ez = m.zint[z];
-                                    Tp = ez >= 0 ? chain_pow(ch, ez) : xpow(X, (T)m.zet[z] - (T)1);
-                                    Tz = Tp * X;
-                                }
+                            for (int z = 0; z < NZ; ++z)
 #pragma unroll
                                 for (int e = 0; e < NE; ++e) {
-                                    SA[e] += wa[(l * NZ + z) * NE + e] * Tz;
-                                    SC[e] += wc[(l * NZ + z) * NE + e] * Tp;
+                                    SA[e] += wa[(l * NZ + z) * NE + e] * Tz[z];
+                                    SC[e] += wc[(l * NZ + z) * NE + e] * Tp[z];
                                 }
-                            }
                         }
                         T A = (T)0, B = (T)0, C = (T)0;
 #pragma unroll
@@ -643,31 +690,32 @@ void set_smem(K kernel, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-template <typename T, int NL, int NZ, int NE>
-void run_shape(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
-    constexpr int P = NL * NZ * NE;
+template <typename T, class S>
+void run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
     const int mm = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
-    const size_t smem = fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, grad) * kWarps;
+    const size_t smem = fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, S::P, grad) * kWarps;
     int blocks = (b.natoms + kWarps - 1) / kWarps;
     const int cap = nsm() * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     if (grad) {
-        set_smem(k_sfg_fast<T, NL, NZ, NE>, smem);
-        k_sfg_fast<T, NL, NZ, NE><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+        set_smem(k_sfg_fast<T, S>, smem);
+        k_sfg_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
     } else {
-        set_smem(k_sfv_fast<T, NL, NZ, NE>, smem);
-        k_sfv_fast<T, NL, NZ, NE><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+        set_smem(k_sfv_fast<T, S>, smem);
+        k_sfv_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
     }
 }
 
 template <typename T>
 void run_any(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
     switch (m.fast) {
-        case 1: run_shape<T, 2, 2, 1>(b, m, grad, st); break;
-        case 2: run_shape<T, 2, 4, 2>(b, m, grad, st); break;
-        case 3: run_shape<T, 2, 4, 4>(b, m, grad, st); break;
-        case 4: run_shape<T, 2, 8, 2>(b, m, grad, st); break;
+        case 1: run_spec<T, Spec<2, 2, 1>>(b, m, grad, st); break;
+        case 2: run_spec<T, Spec<2, 4, 2>>(b, m, grad, st); break;
+        case 3: run_spec<T, Spec<2, 4, 4>>(b, m, grad, st); break;
+        case 4: run_spec<T, Spec<2, 8, 2>>(b, m, grad, st); break;
+        case 5: run_spec<T, Spec<2, 2, 1, 1, 4>>(b, m, grad, st); break;
+        case 6: run_spec<T, Spec<2, 4, 2, 1, 2, 4, 16>>(b, m, grad, st); break;
         default: break;
     }
 }

@@ -79,7 +79,10 @@ int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
 
 /* Context options (for tests and tuning): "generic_sf" = 1 forces the
  * generic symmetry-function kernels (one parameter record per SF) instead of
- * the lambda x zeta x eta kernels; the result is the same within rounding.   */
+ * the lambda x zeta x eta kernels; "runtime_zeta" = 1 makes the
+ * lambda x zeta x eta kernels read the zeta set from the model even when a
+ * kernel with that zeta set compiled in exists.  Results agree within
+ * rounding.                                                                  */
 int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
 
 /* ---------------------------------------------------------------- evaluation

@@ -154,3 +154,16 @@ def test_generic_and_fast_kernels_agree(eng, gab, abx3_model, W):
     assert np.abs(fast["energy"] - gen["energy"]).max() <= E_REL * np.abs(gen["energy"]).max()
     assert np.abs(fast["forces"] - gen["forces"]).max() <= F_ABS
     assert np.abs(fast["dEdLat"] - gen["dEdLat"]).max() <= L_ABS
+
+
+def test_compiled_and_runtime_zeta_kernels_agree(eng, gab, W):
+    s = W.config_c4(n_struct=6, seed=16)
+    fixed = gab.eval_batch(s, dEdLat=True)
+    gab.set_option("runtime_zeta", 1)
+    try:
+        rt = gab.eval_batch(s, dEdLat=True)
+    finally:
+        gab.set_option("runtime_zeta", 0)
+    assert np.abs(fixed["energy"] - rt["energy"]).max() <= E_REL * np.abs(rt["energy"]).max()
+    assert np.abs(fixed["forces"] - rt["forces"]).max() <= F_ABS
+    assert np.abs(fixed["dEdLat"] - rt["dEdLat"]).max() <= L_ABS
