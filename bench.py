@@ -1,22 +1,29 @@
 """Benchmark: atom-steps/s of energy + forces + stress on one or more B200s.
 
-A step is one evaluation (E, F, dE/dh for every structure) of the batched
-mixed-size workload: 4096 independent periodic ABX3 supercells with nx, ny,
-nz uniform in {1..4} (12-768 atoms, about 768k atoms), per-structure strain
-up to 5 % and N(0, 0.15 Bohr) jitter (seed 4 + rank), synthetic 5-element
-potential with 280 symmetry functions per element and 280-25-25-1 networks.
+A step is one evaluation (E, F, dE/dh of every structure) of the batched
+mixed-size workload: 4096 independent periodic ABX3 supercells with nx, ny, nz
+uniform in {1..4} (12-768 atoms, ~759k atoms), per-structure strain up to 5 %
+and N(0, 0.15 Bohr) jitter (seed 4 + rank), synthetic 5-element potential with
+280 symmetry functions per element and 280-25-25-1 networks
+(tests/golden/abx3).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-  python bench.py --impl reference ...   # the CPU restatement on the host cores
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+  python bench.py --impl reference ...   # the reference's algorithm on the host cores
 
-value = atoms x steps / (device time of the K steps, max over ranks), inputs
-resident in HBM (C ABI hdnnp_eval_batch_device); e2e = the same through
-hdnnp_eval_batch with pinned host buffers (H2D of Z/positions/cells and D2H of
-energies/forces/dE/dh inside every timed step).
+value  = atoms x steps / device time of the K steps (max over ranks), inputs
+         resident in HBM, batched path (hdnnp_eval_batch_device), default
+         precision "mixed" (FP32 symmetry functions and networks, FP64 wrap,
+         energy and virial reductions).
+e2e    = the same through hdnnp_eval_batch with pinned host buffers: H2D of
+         Z/positions and D2H of energies/forces/dE/dh inside every step.
+config.compare: the batched FP64 path (same workload) and the plain FP64 form
+         (hdnnp_energy_and_forces, one structure per call, the reference's API)
+         on a sample of the structures, for the north-star ratio.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import subprocess
@@ -40,11 +47,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--structs", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=256, help="structures in the CPU baseline sample")
+    ap.add_argument("--plain-sample", type=int, default=512, help="structures timed through the plain per-structure API")
     ap.add_argument("--lean", action="store_true",
-                    help="device-resident steps only (no e2e, peaks or CPU baseline): for profiler runs")
+                    help="device-resident steps only (no e2e, comparisons, peaks or CPU baseline): for profiler runs")
     return ap.parse_args()
 
 
@@ -98,9 +106,9 @@ class ClockSampler:
 
 
 def measured_peaks(torch):
-    """FP64 and FP32 (no TF32) GEMM throughput of this GPU via cuBLAS (TFLOP/s),
-    the measured denominators for the symmetry-function kernels' CUDA-core
-    arithmetic; HBM and bf16 come from MEASURED_PEAKS.json."""
+    """FP64 and FP32 (no TF32) GEMM throughput of this GPU via cuBLAS (TFLOP/s):
+    the measured CUDA-core denominators for the symmetry-function kernels
+    (MEASURED_PEAKS.json holds only HBM and bf16 tensor peaks)."""
     out = {}
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
@@ -125,12 +133,13 @@ def measured_peaks(torch):
     return out
 
 
-# FP64 operations per work unit of the symmetry-function kernels, counted
-# from the arithmetic in csrc/symfn.cu (additions, multiplications, FMAs as
-# 2; sqrt/exp/tanh/div each counted as one operation).
+# Floating-point operations per work unit of the lambda x zeta x eta
+# symmetry-function kernels for the (2 lambda, zeta {1,2,4,16}, 2 eta) grid of
+# this potential, counted from csrc/symfn_fast.cu (add/mul = 1, FMA = 2,
+# sqrt/exp/tanh/div = 1).  Units come from the engine's counters.
 FLOPS = {
-    "sf_values": {"entries": 25, "pairs": 39, "g4_terms": 10.5, "g2_terms": 6},
-    "sf_gradients": {"entries": 50, "pairs": 151, "g4_terms": 17.5, "g2_terms": 13},
+    "sf_values": {"entries": 30, "pairs": 88, "g2_terms": 6},
+    "sf_gradients": {"entries": 57, "pairs": 263, "g2_terms": 13},
 }
 
 
@@ -163,7 +172,7 @@ def cpu_baseline(structs, sample, seed=0):
 def run_reference(args, rank, world):
     """--impl reference: the reference's algorithm on the host cores.  The
     Fortran reference cannot be built in this image (no Fortran compiler), so
-    its C++ restatement (the oracle, same loops, OpenMP over atoms) runs it."""
+    its C++ restatement (the oracle: same loops, OpenMP over atoms) runs it."""
     if rank != 0:
         return
     W = __graft_entry__.load_package().workloads
@@ -181,7 +190,7 @@ def run_reference(args, rank, world):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": "batched mixed sizes: 4096 periodic ABX3 supercells (12-768 atoms), seed 4",
-                       "step": "E+F+stress of a seeded sample of the structures (atom-steps/s scale-free)"},
+                       "step": "E+F+stress of a seeded sample of the structures (atom-steps/s is size-free)"},
             "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": base["cores"], "kind": "port",
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -212,7 +221,9 @@ def main():
     natoms = int(off[-1])
     nstruct = len(structs)
     pot = engine.Hdnnp.from_runner(POT_DIR, device=local)
-    pot.set_precision(engine.HDNNP_PREC_MIXED if args.precision == "mixed" else engine.HDNNP_PREC_FP64)
+    prec = engine.HDNNP_PREC_MIXED if args.precision == "mixed" else engine.HDNNP_PREC_FP64
+    pot.set_precision(prec)
+    L = engine.lib()
 
     # device-resident inputs / outputs (torch only as the allocator)
     Zd = torch.from_numpy(Z).cuda()
@@ -221,16 +232,13 @@ def main():
     Fd = torch.zeros(natoms, 3, dtype=torch.float64, device="cuda")
     Ld = torch.zeros(nstruct, 9, dtype=torch.float64, device="cuda")
     stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream is NULL)
-    L = engine.lib()
-    import ctypes as C
 
     def step_device():
-        code = L.hdnnp_eval_batch_device(
+        engine._check(L.hdnnp_eval_batch_device(
             pot._c, nstruct, off.ctypes.data_as(C.POINTER(C.c_int64)), None, C.c_void_p(Zd.data_ptr()),
             C.c_void_p(posd.data_ptr()), per.ctypes.data_as(C.POINTER(C.c_int32)),
             latf.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(Ed.data_ptr()), C.c_void_p(Fd.data_ptr()),
-            C.c_void_p(Ld.data_ptr()), C.c_void_p(stream.cuda_stream))
-        engine._check(code)
+            C.c_void_p(Ld.data_ptr()), C.c_void_p(stream.cuda_stream)))
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
 
@@ -238,6 +246,18 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+
+    def timed_device_steps(nsteps):
+        times = []
+        for _ in range(nsteps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_device()
+            e1.record(stream)
+            times.append((e0, e1))
+        return times
 
     # ---------------- value: inputs resident in HBM
     for _ in range(args.warmup):
@@ -247,15 +267,7 @@ def main():
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    times = []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step_device()
-        e1.record(stream)
-        times.append((e0, e1))
+    times = timed_device_steps(args.steps)
     barrier()
     clk = clocks.stop()
     pot.set_profiling(False)
@@ -270,7 +282,8 @@ def main():
     if args.lean:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "ms_per_step": dev_s / args.steps * 1e3,
-                              "stage_ms": stage_ms, "counters": counters, "lean": True}), flush=True)
+                              "precision": args.precision, "stage_ms": stage_ms, "counters": counters,
+                              "lean": True}), flush=True)
         pot.close()
         if world > 1:
             dist.destroy_process_group()
@@ -282,16 +295,14 @@ def main():
     Eh = torch.zeros(nstruct, dtype=torch.float64).pin_memory()
     Fh = torch.zeros(natoms * 3, dtype=torch.float64).pin_memory()
     Lh = torch.zeros(nstruct * 9, dtype=torch.float64).pin_memory()
+    dp = lambda x: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(C.c_double))
 
     def step_host():
-        code = L.hdnnp_eval_batch(
+        engine._check(L.hdnnp_eval_batch(
             pot._c, nstruct, off.ctypes.data_as(C.POINTER(C.c_int64)),
-            C.cast(C.c_void_p(Zh.data_ptr()), C.POINTER(C.c_int32)),
-            C.cast(C.c_void_p(posh.data_ptr()), C.POINTER(C.c_double)), per.ctypes.data_as(C.POINTER(C.c_int32)),
-            latf.ctypes.data_as(C.POINTER(C.c_double)), C.cast(C.c_void_p(Eh.data_ptr()), C.POINTER(C.c_double)),
-            C.cast(C.c_void_p(Fh.data_ptr()), C.POINTER(C.c_double)),
-            C.cast(C.c_void_p(Lh.data_ptr()), C.POINTER(C.c_double)))
-        engine._check(code)
+            C.cast(C.c_void_p(Zh.data_ptr()), C.POINTER(C.c_int32)), dp(posh),
+            per.ctypes.data_as(C.POINTER(C.c_int32)), latf.ctypes.data_as(C.POINTER(C.c_double)),
+            dp(Eh), dp(Fh), dp(Lh)))
 
     for _ in range(max(1, args.warmup // 2)):
         step_host()
@@ -307,7 +318,33 @@ def main():
     e2e_s = float(t.item())
     e2e = natoms * world * args.steps / e2e_s
     h2d = Z.nbytes + pos.nbytes
-    d2h = Eh.numel() * 8 + Fh.numel() * 8 + Lh.numel() * 8
+    d2h = (Eh.numel() + Fh.numel() + Lh.numel()) * 8
+
+    # ---------------- comparisons on the same workload (rank 0)
+    compare = {}
+    if rank == 0:
+        other = engine.HDNNP_PREC_FP64 if prec == engine.HDNNP_PREC_MIXED else engine.HDNNP_PREC_MIXED
+        pot.set_precision(other)
+        step_device()
+        torch.cuda.synchronize()
+        ot = timed_device_steps(max(2, args.steps // 3))
+        torch.cuda.synchronize()
+        osec = sum(a.elapsed_time(b) for a, b in ot) / 1e3
+        compare["batched_" + ("fp64" if other == engine.HDNNP_PREC_FP64 else "mixed")] = natoms * len(ot) / osec
+        pot.set_precision(engine.HDNNP_PREC_FP64)
+        rng = np.random.default_rng(7)
+        idx = rng.choice(nstruct, size=min(args.plain_sample, nstruct), replace=False)
+        sample = [engine.AtStruct(structs[int(k)]["Z"], structs[int(k)]["pos"], structs[int(k)]["lat"]) for k in idx]
+        pot.energy_and_forces(sample[0], dEdLat=True)
+        atoms = sum(a.nat for a in sample)
+        t0 = time.perf_counter()
+        for a in sample:
+            pot.energy_and_forces(a, dEdLat=True)
+        psec = time.perf_counter() - t0
+        compare["plain_fp64_per_structure"] = atoms / psec
+        compare["plain_sample"] = f"{len(sample)} structures ({atoms} atoms), hdnnp_energy_and_forces with host arrays"
+        compare["value_over_plain_fp64"] = value / compare["plain_fp64_per_structure"]
+        pot.set_precision(prec)
 
     # ---------------- roofline of the dominant kernel
     evals = max(counters["evaluations"], 1)
@@ -317,11 +354,10 @@ def main():
     peaks = measured_peaks(torch) if rank == 0 else {}
     peak_key = "fp64" if args.precision == "fp64" else "fp32"
     achieved = flops / (dom_ms / 1e3) / 1e12
-    roof = {"bound": peak_key, "kernel": dom, "achieved": achieved, "peak": peaks.get(peak_key),
+    roof = {"bound": peak_key + "-alu", "kernel": dom, "achieved": achieved, "peak": peaks.get(peak_key),
             "unit": "TFLOP/s", "frac": achieved / peaks[peak_key] if peaks.get(peak_key) else None,
             "peak_source": f"measured in this run: cuBLAS {peak_key.upper()} GEMM (no TF32), best of 5",
-            "traffic": None,
-            "flops_per_launch": flops, "ms_per_launch": dom_ms,
+            "traffic": None, "flops_per_launch": flops, "ms_per_launch": dom_ms,
             "stage_ms_per_step": {k: v / evals for k, v in stage_ms.items()},
             "units_per_step": {k: v / evals for k, v in counters.items() if k != "evaluations"}}
 
@@ -332,14 +368,15 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_s / args.steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32+fp16",
+                "dtype": "f64" if args.precision == "fp64" else "f32 (f64 wrap/energy/virial)",
                 "data": "synthetic (seeded ABX3 supercells, random-init 280-SF potential)",
                 "config": {"workload": f"batched mixed sizes: {nstruct} periodic ABX3 supercells per GPU "
                                        f"(12-768 atoms, {natoms} atoms, seed 4+rank), E+F+stress",
                            "global_batch": natoms * world, "precision": args.precision,
                            "parallelism": f"replicas x{world} (independent structures per GPU)",
                            "l2": "256 MB buffer written between timed steps; working set (G alone "
-                                 f"{natoms * 280 * 8 / 1e9:.1f} GB) is larger than L2"},
+                                 f"{natoms * 280 * 4 / 1e9:.1f}+ GB) is larger than L2",
+                           "compare": compare},
                 "e2e": {"value": e2e, "unit": "atom-steps/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": launches_per_step * args.steps,

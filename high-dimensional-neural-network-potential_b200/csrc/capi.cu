@@ -1,5 +1,6 @@
 // capi.cu -- C ABI of the engine (include/hdnnp_gpu.h): model upload,
 // evaluation contexts, host-side structure set-up and the stage pipeline.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -175,6 +176,7 @@ struct hdnnp_ctx {
     int precision = HDNNP_PREC_FP64;
     int generic_sf = 0;
     int runtime_zeta = 0;
+    int mlp_simt = 0;
     int launches = 0;
     // device buffers
     DevBuf<StructInfo> info;
@@ -406,8 +408,68 @@ int upload_model(hdnnp_model* m) {
            o_wo = add(w_off.data(), w_off.size() * 8), o_bo = add(b_off.data(), b_off.size() * 8),
            o_ae = add(ae.data(), ae.size() * 8);
     std::vector<float> wf(w.begin(), w.end()), wtf(wt.begin(), wt.end()), bf(bias.begin(), bias.end());
+
+    // First layer for the tensor-core network kernel: scale W1 by a power of
+    // two (max |s1 W1| in [1, 2)), split into FP16 hi + lo, pack K-major
+    // core matrices (8 rows x 16 B, row groups 128 B apart, K chunks of 8).
+    std::vector<unsigned short> tcf, tcb;
+    {
+        const int kH = 32;
+        bool ok = L >= 2 && L <= 4;
+        for (int l = 0; l < L && ok; ++l) ok = D.width[l + 1] <= kH;
+        const int kp = (nsf_max + 15) / 16 * 16;
+        int np = kp;
+        const int nch = (np + 255) / 256;
+        const int chn = ((np + nch - 1) / nch + 15) / 16 * 16;
+        np = nch * chn;
+        ok = ok && (kH + np) <= 512 && kp <= 512;
+        const size_t szA = (size_t)2 * 128 * kp * 2, szBf = (size_t)2 * kH * kp * 2, szBb = (size_t)2 * np * kH * 2,
+                     szAb = (size_t)2 * 128 * kH * 2;
+        size_t wsmall = D.width[1];
+        for (int l = 1; l < L; ++l) wsmall += (size_t)D.width[l + 1] * D.width[l] + D.width[l + 1];
+        const size_t total = std::max(szA, szBb + szAb) + szBf + ((wsmall * 4 + 15) & ~size_t(15)) + 64;
+        ok = ok && total <= 227 * 1024;
+        if (ok) {
+            auto cm = [](int row, int k, int rows) {
+                return (size_t)((k >> 3) * (rows >> 3) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2) / 2;
+            };
+            const size_t fper = (size_t)kH * kp, bper = (size_t)np * kH;  // halfwords per hi (or lo) part
+            tcf.assign((size_t)nel * 2 * fper, 0);
+            tcb.assign((size_t)nel * 2 * bper, 0);
+            for (int c = 0; c < nel; ++c) {
+                const Layer& l0 = H.el[c].net[0];
+                double mx = 0.0;
+                for (double v : l0.w) mx = std::max(mx, std::fabs(v));
+                const double s1 = mx > 0 ? std::ldexp(1.0, -(int)std::floor(std::log2(mx))) : 1.0;
+                D.tc_inv_s1[c] = (float)(1.0 / s1);
+                unsigned short* F = tcf.data() + (size_t)c * 2 * fper;
+                unsigned short* B = tcb.data() + (size_t)c * 2 * bper;
+                for (int n = 0; n < l0.nout; ++n)
+                    for (int k = 0; k < l0.nin; ++k) {
+                        const double wv = l0.w[(size_t)n * l0.nin + k] * s1;
+                        const __half hi = __float2half_rn((float)wv);
+                        const __half lo = __float2half_rn((float)(wv - (double)__half2float(hi)));
+                        const unsigned short uh = __half_as_ushort(hi), ul = __half_as_ushort(lo);
+                        F[cm(n, k, kH)] = uh;
+                        F[fper + cm(n, k, kH)] = ul;
+                        B[cm(k, n, np)] = uh;  // transposed: row = input index, K = hidden index
+                        B[bper + cm(k, n, np)] = ul;
+                    }
+            }
+            D.tc_ok = 1;
+            D.tc_kp = kp;
+            D.tc_np = np;
+            D.tc_nch = nch;
+            D.tc_chn = chn;
+            D.tc_sdelta = 64.0f;
+        } else {
+            tcf.assign(8, 0);
+            tcb.assign(8, 0);
+        }
+    }
     size_t o_pm = add(pmap.data(), pmap.size() * sizeof(short)), o_wf = add(wf.data(), wf.size() * 4),
-           o_wtf = add(wtf.data(), wtf.size() * 4), o_bf = add(bf.data(), bf.size() * 4);
+           o_wtf = add(wtf.data(), wtf.size() * 4), o_bf = add(bf.data(), bf.size() * 4),
+           o_tcf = add(tcf.data(), tcf.size() * 2), o_tcb = add(tcb.data(), tcb.size() * 2);
     CUDA_TRY(cudaSetDevice(m->device));
     CUDA_TRY(cudaMalloc(&m->dmem, off));
     char* base = (char*)m->dmem;
@@ -431,6 +493,8 @@ int upload_model(hdnnp_model* m) {
     D.wf = (const float*)(base + o_wf);
     D.wtf = (const float*)(base + o_wtf);
     D.bf = (const float*)(base + o_bf);
+    D.tc_fwd = (const unsigned short*)(base + o_tcf);
+    D.tc_bwd = (const unsigned short*)(base + o_tcb);
     return HDNNP_OK;
 }
 
@@ -440,6 +504,7 @@ int check_status(hdnnp_ctx* c) {
     if (f & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
     if (f & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
     if (f & 8) return fail(HDNNP_E_INPUT, "non-finite position");
+    if (f & 16) return fail(HDNNP_E_TIMEOUT, "tensor-core network kernel: bounded wait expired");
     return HDNNP_OK;
 }
 
@@ -583,7 +648,10 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if ((r = mark(3))) return r;
     L += fast ? launch_sf_values_fast(b, D, mixed, st) : launch_sf_values(b, D, st);
     if ((r = mark(4))) return r;
-    L += mixed ? launch_mlp_fp32(b, D, st) : launch_mlp(b, D, st);
+    if (mixed && D.tc_ok && !c->mlp_simt)
+        L += launch_mlp_tc(b, D, st);
+    else
+        L += mixed ? launch_mlp_fp32(b, D, st) : launch_mlp(b, D, st);
     if ((r = mark(5))) return r;
     L += fast ? launch_sf_gradients_fast(b, D, mixed, st) : launch_sf_gradients(b, D, st);
     if ((r = mark(6))) return r;
@@ -700,6 +768,10 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
     if (!c || !name) return fail(HDNNP_E_INPUT, "null argument");
     if (std::string(name) == "generic_sf") {
         c->generic_sf = value != 0;
+        return HDNNP_OK;
+    }
+    if (std::string(name) == "mlp_simt") {
+        c->mlp_simt = value != 0;
         return HDNNP_OK;
     }
     if (std::string(name) == "runtime_zeta") {

@@ -96,6 +96,16 @@ struct DevModel {
     const float* wf;
     const float* wtf;
     const float* bf;
+    // First layer packed for the tensor-core network kernel (mlp_tc.cu):
+    // FP16 hi | lo of s1 * W1 per element in the K-major core-matrix layouts
+    // of the forward GEMM (32 x tc_kp) and of the input-gradient GEMM
+    // (tc_np x 32).  tc_ok = 0 if the network does not fit the kernel.
+    int tc_ok;
+    int tc_kp, tc_np, tc_nch, tc_chn;
+    float tc_sdelta;              // power-of-two scale of delta1 before the split
+    float tc_inv_s1[kMaxEl];      // 1 / s1 per element
+    const unsigned short* tc_fwd;
+    const unsigned short* tc_bwd;
 };
 
 // Workspace pointers for one batch evaluation (all device memory).
@@ -167,6 +177,8 @@ int launch_element_groups(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_mlp_fp32(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_forces_and_reduce_fp32(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s);
 size_t mlp_smem_bytes(const DevModel& m, size_t elem);
+int launch_mlp_tc(const Batch& b, const DevModel& m, cudaStream_t s);
+size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
 

@@ -1,0 +1,460 @@
+// mlp_tc.cu -- K5 of the mixed-precision form: per-element atomic networks
+// with the first layer on the 5th-generation tensor cores (tcgen05).
+//
+// Same mathematics as nn_forward / nn_backward(gradOut = 1)
+// (neuralNetworks.f90:94-158, 220-313; called per atom from
+// hdnnps.f90:523-531).  One CTA evaluates a tile of 128 atoms of one element;
+// thread m owns atom m, which is also TMEM lane m.
+//   forward layer 1:  C1[128 x H] = G'[128 x K] W1^T        (tcgen05.mma, M=128)
+//   layers 2..L:      per thread in FP32 registers (widths <= 32)
+//   input gradient:   dE/dG'[128 x N] = delta1[128 x H] W1   (tcgen05.mma, N split
+//                     into chunks of <= 256 columns)
+// Both GEMMs run in FP16 with FP32 accumulation and a hi + lo split of both
+// operands (x = hi + lo, both FP16): A B = Ahi Bhi + Ahi Blo + Alo Bhi, which
+// carries about 22 significant bits, so the input gradient that sets the
+// forces keeps FP32-level accuracy.  Weights are pre-scaled by a power of two
+// (so that their lo parts stay normal FP16 numbers) and pre-packed at model
+// upload in the K-major, no-swizzle core-matrix layout the MMA descriptors
+// describe: 8 rows x 16 bytes per core matrix, rows 16 B apart, row groups
+// (SBO) 128 B apart, K chunks of 8 elements (LBO) one row-group column apart.
+// Operands are staged into shared memory with plain loads (the activations
+// are converted FP32 -> FP16 hi/lo on the way), MMAs are issued by one
+// thread, completion is signalled through an mbarrier by tcgen05.commit, and
+// results are read back with tcgen05.ld.  Every mbarrier wait is bounded;
+// on expiry the kernel raises status bit 16 and frees its TMEM.
+#include <cuda_fp16.h>
+
+#include "engine.h"
+
+namespace hdnnp {
+
+namespace {
+
+constexpr int kM = 128;        // atoms per tile (TMEM lanes, MMA M)
+constexpr int kThr = 128;      // threads per CTA (4 warps; thread = row)
+constexpr int kH = 32;         // padded hidden width (N of GEMM 1, K of GEMM 2)
+constexpr int kTmemCols = 512;
+constexpr long long kWaitIters = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start, leading (K) and stride (M/N) byte
+// offsets in 16-byte units, version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// instruction descriptor: FP16 x FP16 -> FP32, both operands K-major
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (long long it = 0; it < kWaitIters; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// byte offset of element (row, k) in a K-major core-matrix tile with `rows` rows
+__device__ __forceinline__ uint32_t cm_off(int row, int k, int rows) {
+    return (uint32_t)((k >> 3) * (rows >> 3) * 128 + (row >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void split_h(float x, __half& hi, __half& lo) {
+    hi = __float2half_rn(x);
+    lo = __float2half_rn(x - __half2float(hi));
+}
+
+__device__ __forceinline__ float act_fw(char a, float x) {
+    switch (a) {
+        case 't': return tanhf(x);
+        case 'p': return log1pf(expf(x));
+        case 'r': return x > 0.f ? x : 0.f;
+        default: return x;
+    }
+}
+__device__ __forceinline__ float act_dv(char a, float c, float y) {
+    switch (a) {
+        case 't': return 1.f - y * y;
+        case 'p': return 1.f / (1.f + expf(-c));
+        case 'r': return c > 0.f ? 1.f : 0.f;
+        default: return 1.f;
+    }
+}
+
+// Shared-memory plan (bytes):
+//   [0, szA)            A_fwd hi | lo  (128 x Kp each); reused for B_bwd hi|lo and A_bwd hi|lo
+//   [szA, szA+szBf)     B_fwd hi | lo  (32 x Kp each)
+//   then FP32 small weights of layers 2..L, then the mbarrier and the TMEM slot
+struct TCPlan {
+    int Kp, Np, nch, chN;
+    size_t szA, szBf, szBb, szAb, szW, total;
+};
+
+__host__ __device__ inline TCPlan tc_plan(const DevModel& m) {
+    TCPlan p{};
+    p.Kp = m.tc_kp;
+    p.Np = m.tc_np;
+    p.nch = m.tc_nch;
+    p.chN = m.tc_chn;
+    p.szA = (size_t)2 * kM * p.Kp * 2;
+    p.szBf = (size_t)2 * kH * p.Kp * 2;
+    p.szBb = (size_t)2 * p.Np * kH * 2;
+    p.szAb = (size_t)2 * kM * kH * 2;
+    size_t w = 0;
+    for (int l = 1; l < m.nlayers; ++l) w += (size_t)m.width[l + 1] * m.width[l] + m.width[l + 1];
+    w += m.width[1];  // b1
+    p.szW = ((w * 4) + 15) & ~size_t(15);
+    size_t reuse = p.szBb + p.szAb;
+    p.total = (p.szA > reuse ? p.szA : reuse) + p.szBf + p.szW + 64;
+    return p;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const TCPlan P = tc_plan(m);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // locate (element, tile)
+    int tile = blockIdx.x, e = -1, t0 = 0, cnt = 0;
+    for (int x = 0; x < m.nel; ++x) {
+        const int n = b.el_start[x + 1] - b.el_start[x];
+        const int nt = (n + kM - 1) / kM;
+        if (tile < nt) {
+            e = x;
+            t0 = b.el_start[x] + tile * kM;
+            cnt = min(kM, n - tile * kM);
+            break;
+        }
+        tile -= nt;
+    }
+    if (e < 0) return;
+    const int nin = m.nin_el[e];
+    const int H = m.width[1];
+    constexpr int L = NL;
+    unsigned char* sA = sm;
+    unsigned char* sBf = sm + (P.szA > P.szBb + P.szAb ? P.szA : P.szBb + P.szAb);
+    float* sW = (float*)(sBf + P.szBf);
+    uint64_t* mbar = (uint64_t*)((unsigned char*)sW + P.szW);
+    uint32_t* tslot = (uint32_t*)(mbar + 1);
+    const uint32_t mb = smem_u32(mbar);
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+
+    // ---- stage B_fwd (pre-packed hi|lo) and the small FP32 weights
+    {
+        const uint4* src = (const uint4*)(m.tc_fwd + (size_t)e * (P.szBf / 2));
+        uint4* dst = (uint4*)sBf;
+        for (int i = tid; i < (int)(P.szBf / 16); i += kThr) dst[i] = src[i];
+        int o = 0;
+        const float* b1 = m.bf + m.b_off[e * L + 0];
+        for (int i = tid; i < H; i += kThr) sW[i] = b1[i];
+        o += H;
+        for (int l = 1; l < L; ++l) {
+            const int wi = m.width[l], wo = m.width[l + 1];
+            const float* W = m.wf + m.w_off[e * L + l];
+            const float* bb = m.bf + m.b_off[e * L + l];
+            for (int i = tid; i < wi * wo; i += kThr) sW[o + i] = W[i];
+            o += wi * wo;
+            for (int i = tid; i < wo; i += kThr) sW[o + i] = bb[i];
+            o += wo;
+        }
+    }
+    // ---- stage A_fwd: thread = row; its row of G' (FP32) -> FP16 hi | lo in
+    // groups of 4 k (one 8-byte store per part), zero padding.  32 values are
+    // loaded before any is stored, so each thread keeps 8 vector loads in flight.
+    {
+        __half* Ahi = (__half*)sA;
+        __half* Alo = (__half*)(sA + P.szA / 2);
+        const int kp = P.Kp;
+        const int r = tid;
+        const int at = r < cnt ? b.el_atoms[t0 + r] : -1;
+        const float* row = at >= 0 ? b.Gf + (size_t)at * m.nsf_max : nullptr;
+        const bool vec = (m.nsf_max & 3) == 0;
+        for (int k0 = 0; k0 < kp; k0 += 32) {
+            float x[32];
+            if (vec && at >= 0) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int k = k0 + 4 * q;
+                    float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (k + 3 < nin) f = *(const float4*)(row + k);
+                    else {
+                        if (k < nin) f.x = row[k];
+                        if (k + 1 < nin) f.y = row[k + 1];
+                        if (k + 2 < nin) f.z = row[k + 2];
+                    }
+                    x[4 * q] = f.x; x[4 * q + 1] = f.y; x[4 * q + 2] = f.z; x[4 * q + 3] = f.w;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) x[q] = (at >= 0 && k0 + q < nin) ? row[k0 + q] : 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = k0 + 4 * q;
+                if (k < kp) {
+                    __half h[4], l[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) split_h(x[4 * q + u], h[u], l[u]);
+                    const uint32_t off = cm_off(r, k, kM);
+                    auto pk = [](const __half (&v)[4]) {
+                        return make_uint2((uint32_t)__half_as_ushort(v[0]) | ((uint32_t)__half_as_ushort(v[1]) << 16),
+                                          (uint32_t)__half_as_ushort(v[2]) | ((uint32_t)__half_as_ushort(v[3]) << 16));
+                    };
+                    *(uint2*)((unsigned char*)Ahi + off) = pk(h);
+                    *(uint2*)((unsigned char*)Alo + off) = pk(l);
+                }
+            }
+        }
+    }
+    fence_async_smem();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    bool ok = true;
+
+    // ---- GEMM 1: C1[128 x 32] = A_fwd * B_fwd^T  (K = Kp in steps of 16)
+    if (tid == 0) {
+        const uint32_t aH = smem_u32(sA), aL = aH + (uint32_t)(P.szA / 2);
+        const uint32_t bH = smem_u32(sBf), bL = bH + (uint32_t)(P.szBf / 2);
+        const uint32_t lboA = (kM / 8) * 128, lboB = (kH / 8) * 128;
+        const uint32_t id = idesc_f16(kM, kH);
+        for (int s = 0; s < P.Kp / 16; ++s) {
+            const uint32_t oa = (uint32_t)(2 * s) * lboA, ob = (uint32_t)(2 * s) * lboB;
+            mma_f16(tbase, umma_desc(aH + oa, lboA, 128), umma_desc(bH + ob, lboB, 128), id, s > 0);
+            mma_f16(tbase, umma_desc(aH + oa, lboA, 128), umma_desc(bL + ob, lboB, 128), id, 1);
+            mma_f16(tbase, umma_desc(aL + oa, lboA, 128), umma_desc(bH + ob, lboB, 128), id, 1);
+        }
+        mma_commit(mb);
+    }
+    ok = mbar_wait(mb, 0);
+    tc_fence_after();
+
+    const int row = tid;
+    const bool live = row < cnt;
+    const int atom = live ? b.el_atoms[t0 + row] : 0;
+    if (ok) {
+        // offsets of the FP32 weights of layers 1..L-1 in sW
+        int woff[NL], boff[NL];
+        {
+            int o = H;
+#pragma unroll
+            for (int l = 1; l < NL; ++l) {
+                woff[l] = o;
+                o += m.width[l] * m.width[l + 1];
+                boff[l] = o;
+                o += m.width[l + 1];
+            }
+        }
+        float v[32];
+        tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), v);
+        const float inv = m.tc_inv_s1[e];
+        float yp[kH];          // activations of the previous layer
+        float dact[NL][kH];    // act'(c) of every layer, for the backward pass
+#pragma unroll
+        for (int o = 0; o < kH; ++o) {
+            const float c = o < H ? v[o] * inv + sW[o] : 0.f;
+            const float yv = o < H ? act_fw(m.act[0], c) : 0.f;
+            yp[o] = yv;
+            dact[0][o] = o < H ? act_dv(m.act[0], c, yv) : 0.f;
+        }
+#pragma unroll
+        for (int l = 1; l < NL; ++l) {
+            const int wi = m.width[l], wo = m.width[l + 1];
+            const float* W = sW + woff[l];
+            const float* bb = sW + boff[l];
+            const char al = m.act[l];
+            float yc[kH];
+#pragma unroll
+            for (int o = 0; o < kH; ++o) {
+                float c = 0.f;
+                if (o < wo) {
+                    c = bb[o];
+#pragma unroll
+                    for (int i = 0; i < kH; ++i)
+                        if (i < wi) c += W[o * wi + i] * yp[i];
+                }
+                const float yv = o < wo ? act_fw(al, c) : 0.f;
+                yc[o] = yv;
+                dact[l][o] = o < wo ? act_dv(al, c, yv) : 0.f;
+            }
+#pragma unroll
+            for (int o = 0; o < kH; ++o) yp[o] = yc[o];
+        }
+        if (live) b.atEf[atom] = (float)((double)yp[0] + m.atom_energy[e]);
+        // backward (gradOut = 1) down to the first hidden layer
+        float d[kH];
+#pragma unroll
+        for (int o = 0; o < kH; ++o) d[o] = dact[NL - 1][o];
+#pragma unroll
+        for (int l = NL - 1; l >= 1; --l) {
+            const int wi = m.width[l], wo = m.width[l + 1];
+            const float* W = sW + woff[l];
+            float g[kH];
+#pragma unroll
+            for (int i = 0; i < kH; ++i) {
+                float sacc = 0.f;
+                if (i < wi) {
+#pragma unroll
+                    for (int o = 0; o < kH; ++o)
+                        if (o < wo) sacc += W[o * wi + i] * d[o];
+                }
+                g[i] = sacc * dact[l - 1][i];
+            }
+#pragma unroll
+            for (int i = 0; i < kH; ++i) d[i] = g[i];
+        }
+        // ---- stage A_bwd (delta1 scaled, hi | lo) and B_bwd in the A_fwd region
+        __half* Bhi = (__half*)sA;
+        __half* Ahi = (__half*)(sA + P.szBb);
+        __half* Alo = (__half*)(sA + P.szBb + P.szAb / 2);
+        const float sd = m.tc_sdelta;
+#pragma unroll
+        for (int k = 0; k < kH; ++k) {
+            __half h, lo;
+            split_h(live ? d[k] * sd : 0.f, h, lo);
+            const uint32_t o2 = cm_off(row, k, kM) >> 1;
+            Ahi[o2] = h;
+            Alo[o2] = lo;
+        }
+        const uint4* src = (const uint4*)(m.tc_bwd + (size_t)e * (P.szBb / 2));
+        uint4* dst = (uint4*)Bhi;
+        for (int i = tid; i < (int)(P.szBb / 16); i += kThr) dst[i] = src[i];
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const int okall = __syncthreads_and(ok ? 1 : 0);
+
+    // ---- GEMM 2: dE/dG'[128 x Np] = A_bwd * B_bwd^T (K = 32, N in chunks)
+    if (okall) {
+        if (tid == 0) {
+            const uint32_t bH = smem_u32(sA), bL = bH + (uint32_t)(P.szBb / 2);
+            const uint32_t aH = smem_u32(sA) + (uint32_t)P.szBb, aL = aH + (uint32_t)(P.szAb / 2);
+            const uint32_t lboA = (kM / 8) * 128, lboB = (uint32_t)(P.Np / 8) * 128;
+            const uint32_t id = idesc_f16(kM, P.chN);
+            for (int c = 0; c < P.nch; ++c) {
+                const uint32_t dcol = tbase + kH + (uint32_t)(c * P.chN);
+                const uint32_t boff = (uint32_t)(c * P.chN / 8) * 128;
+                for (int s = 0; s < kH / 16; ++s) {
+                    const uint32_t oa = (uint32_t)(2 * s) * lboA, ob = (uint32_t)(2 * s) * lboB + boff;
+                    mma_f16(dcol, umma_desc(aH + oa, lboA, 128), umma_desc(bH + ob, lboB, 128), id, s > 0);
+                    mma_f16(dcol, umma_desc(aH + oa, lboA, 128), umma_desc(bL + ob, lboB, 128), id, 1);
+                    mma_f16(dcol, umma_desc(aL + oa, lboA, 128), umma_desc(bH + ob, lboB, 128), id, 1);
+                }
+            }
+            mma_commit(mb);
+        }
+        ok = mbar_wait(mb, 1);
+        tc_fence_after();
+        if (ok) {
+            const float inv = m.tc_inv_s1[e] / m.tc_sdelta;
+            float* out = b.dEdGf + (size_t)atom * m.nsf_max;
+            for (int c0 = 0; c0 < P.nch * P.chN; c0 += 32) {
+                float v[32];
+                tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kH + c0), v);
+                if (live) {
+                    if ((m.nsf_max & 3) == 0 && c0 + 32 <= nin) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            *(float4*)(out + c0 + 4 * q) = make_float4(v[4 * q] * inv, v[4 * q + 1] * inv,
+                                                                       v[4 * q + 2] * inv, v[4 * q + 3] * inv);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 32; ++i)
+                            if (c0 + i < nin) out[c0 + i] = v[i] * inv;
+                    }
+                }
+            }
+        }
+    }
+    if (!ok && tid == 0) atomicOr(&b.status[0], 16);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+    }
+}
+
+}  // namespace
+
+size_t mlp_tc_smem_bytes(const DevModel& m) { return tc_plan(m).total; }
+
+template <int NL>
+void run_tc(const Batch& b, const DevModel& m, cudaStream_t s) {
+    const size_t smem = tc_plan(m).total;
+    cudaFuncSetAttribute(k_mlp_tc<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int tiles = b.natoms / kM + m.nel + 1;
+    k_mlp_tc<NL><<<tiles, kThr, smem, s>>>(b, m);
+}
+
+int launch_mlp_tc(const Batch& b, const DevModel& m, cudaStream_t s) {
+    switch (m.nlayers) {
+        case 2: run_tc<2>(b, m, s); break;
+        case 3: run_tc<3>(b, m, s); break;
+        case 4: run_tc<4>(b, m, s); break;
+        default: return 0;
+    }
+    return 1;
+}
+
+}  // namespace hdnnp

@@ -75,3 +75,19 @@ def test_mixed_alone_equals_in_mix(gmix, W):
         alone = gmix.eval_batch([structs[k]], dEdLat=True)
         assert abs(alone["energy"][0] - mix["energy"][k]) <= 1e-9 * len(structs[k]["Z"])
         assert np.abs(alone["forces"] - mix["forces"][off[k]:off[k + 1]]).max() <= 1e-9
+
+
+def test_tensor_core_network_matches_simt(gmix, W):
+    """tcgen05 FP16 hi+lo network (default) vs the FP32 CUDA-core network."""
+    s = W.config_c4(n_struct=10, seed=17)
+    tc = gmix.eval_batch(s, dEdLat=True)
+    gmix.set_option("mlp_simt", 1)
+    try:
+        simt = gmix.eval_batch(s, dEdLat=True)
+    finally:
+        gmix.set_option("mlp_simt", 0)
+    nat = np.array([len(x["Z"]) for x in s])
+    dE = np.abs(tc["energy"] - simt["energy"]) / nat
+    dF = np.abs(tc["forces"] - simt["forces"]).max()
+    print(f"tensor-core vs SIMT network: |dE|/atom {dE.max():.2e}  max|dF| {dF:.2e}")
+    assert dE.max() <= 1e-6 and dF <= 1e-5
