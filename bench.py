@@ -39,6 +39,11 @@ import __graft_entry__  # noqa: E402
 
 POT_DIR = os.path.join(ROOT, "tests", "golden", "abx3")
 METRIC = "atom-steps/s (E+F+stress)"
+# MD time step of the served walkers (a.u.).  The random-init potential is
+# stiff: velocity Verlet at the example's 20 a.u. heats its trajectories until
+# positions become non-finite within a few hundred steps; at 0.5 a.u. the total
+# energy stays bounded over thousands of steps.
+DT_SYNTH = 0.5
 
 
 def parse():
@@ -51,6 +56,8 @@ def parse():
     ap.add_argument("--structs", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=256, help="structures in the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=512, help="structures timed through the plain per-structure API")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="seconds per load point of the serving leg (0: skip)")
     ap.add_argument("--lean", action="store_true",
                     help="device-resident steps only (no e2e, comparisons, peaks or CPU baseline): for profiler runs")
     return ap.parse_args()
@@ -195,6 +202,48 @@ def run_reference(args, rank, world):
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def serve_leg(pkg, engine, pot, prec, seconds):
+    """Served walkers: 256 ABX3 supercell walkers of 96-3072 atoms (seed 5),
+    half velocity-Verlet MD (300 K, dt 20 a.u.), half Metropolis MC
+    (N(0, 0.05 Bohr) trial moves), resident on the device in one server
+    (2 workers, 131,072-atom batches, 32 GB HBM budget).  A closed-loop
+    point (every idle walker steps at once) gives the saturated throughput;
+    Poisson arrivals at 25/50/80 % of it give latency under load."""
+    from hdnnp_b200 import server as S
+
+    W = pkg.workloads
+    walkers = W.config_c5()
+    budget = 32 << 30
+    srv = S.Server(pot, max_batch_atoms=131072, workers=2, precision=prec, hbm_budget=budget)
+    info = []
+    for k, s in enumerate(walkers):
+        md = k % 2 == 0
+        m, p = W.maxwell_boltzmann(s["Z"], 300.0, 1000 + k) if md else (None, None)
+        init = dict(Z=s["Z"], pos=s["pos"], lat=s["lat"], masses=m, momenta=p)
+        info.append((srv.add_walker(**init), len(s["Z"]), md, init))
+    ts = [srv.submit(w[0], S.REQ_EVAL) for w in info]
+    for t in ts:
+        srv.wait(t)
+    S.poisson_load(srv, info, None, min(1.0, seconds), seed=50, dt=DT_SYNTH)  # warm-up (workspaces grow)
+    srv.stats(reset=True)
+
+    def point(rate, seed):
+        r = S.poisson_load(srv, info, rate, seconds, seed=seed, dt=DT_SYNTH)
+        r["mean_batch_requests"] = srv.stats(reset=True)["mean_batch_requests"]
+        f = r.pop("failed_walkers")
+        r["restarts"] = len(f)  # trajectories restarted after their positions became non-finite
+        return r
+
+    sat = point(None, 51)
+    sweep = [point(frac * sat["steps_per_s"], 52 + k) for k, frac in enumerate((0.25, 0.5, 0.8))]
+    hbm = srv.stats()["hbm_charged"]
+    srv.close()
+    nat = [w[1] for w in info]
+    return {"workload": f"{len(info)} walkers, {min(nat)}-{max(nat)} atoms ({sum(nat)} total), half MD half MC",
+            "server": "2 workers, 131072-atom batches", "hbm_budget": budget, "hbm_charged": hbm,
+            "saturation": sat, "poisson_sweep": sweep}
 
 
 def main():
@@ -345,6 +394,10 @@ def main():
         compare["plain_sample"] = f"{len(sample)} structures ({atoms} atoms), hdnnp_energy_and_forces with host arrays"
         compare["value_over_plain_fp64"] = value / compare["plain_fp64_per_structure"]
         pot.set_precision(prec)
+        if world == 1 and args.serve_seconds > 0:
+            compare["served"] = serve_leg(pkg, engine, pot, prec, args.serve_seconds)
+            compare["served_over_plain_fp64"] = (compare["served"]["saturation"]["atom_steps_per_s"]
+                                                 / compare["plain_fp64_per_structure"])
 
     # ---------------- roofline of the dominant kernel
     evals = max(counters["evaluations"], 1)

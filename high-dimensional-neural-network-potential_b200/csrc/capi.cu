@@ -503,7 +503,8 @@ int check_status(hdnnp_ctx* c) {
     if (f & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
     if (f & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
     if (f & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
-    if (f & 8) return fail(HDNNP_E_INPUT, "non-finite position");
+    if (f & 8)
+        return fail(HDNNP_E_INPUT, "non-finite position (structure " + std::to_string(c->h_status[1] - 1) + ")");
     if (f & 16) return fail(HDNNP_E_TIMEOUT, "tensor-core network kernel: bounded wait expired");
     return HDNNP_OK;
 }
@@ -601,6 +602,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     CUDA_TRY(cudaMemcpyAsync(c->h_status + 2, b.nei_off + natoms, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(c->h_status + 3, b.status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(c->h_status + 1, b.status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     if ((r = check_status(c))) return r;
     tot_max[0] = c->h_status[2];
@@ -1087,3 +1089,46 @@ extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, co
     if (h[0] & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
     return HDNNP_OK;
 }
+
+// ====================================================================== internal (C++) entry points of the server
+namespace hdnnp {
+
+int model_device(const hdnnp_model* m) { return m->device; }
+
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+// Device-resident batch (as hdnnp_eval_batch_device) in which molecules are
+// allowed: mol_pos[s] is a host copy of a non-periodic structure's positions,
+// read only for its bounding box (null for periodic structures).
+int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* Z_dev, const double* pos_dev,
+                  const double* const* mol_pos, const int32_t* periodic, const double* lat, double* energy_dev,
+                  double* force_dev, double* dEdLat_dev, cudaStream_t st) {
+    if (!c || nstruct <= 0 || !off || !Z_dev || !pos_dev || !periodic || !lat || !energy_dev || !force_dev)
+        return fail(HDNNP_E_INPUT, "null argument or empty batch");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    const HostModel& H = c->model->host;
+    c->hinfo.resize(nstruct);
+    if (off[0] != 0) return fail(HDNNP_E_INPUT, "atom_off[0] must be 0");
+    for (int s = 0; s < nstruct; ++s) {
+        const int64_t a0 = off[s], a1 = off[s + 1];
+        if (a1 <= a0) return fail(HDNNP_E_INPUT, "structure " + std::to_string(s) + " has no atoms");
+        const double* mp = periodic[s] ? nullptr : (mol_pos ? mol_pos[s] : nullptr);
+        int r = struct_setup((int)(a1 - a0), mp, periodic[s], lat + 9 * s, H.max_rc, c->hinfo[s]);
+        if (r) return fail(r, "structure " + std::to_string(s) + ": " + g_err);
+        c->hinfo[s].atom_off = (int)a0;
+        c->hinfo[s].nat = (int)(a1 - a0);
+    }
+    return run_pipeline(c, nstruct, (int)off[nstruct], Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st);
+}
+
+// Device error flags of the last evaluation on c (valid after its stream has
+// been synchronised).
+int ctx_check_status(hdnnp_ctx* c) { return check_status(c); }
+
+// Batch index of a structure with a non-finite position in the last
+// evaluation on c, or -1.
+int ctx_bad_struct(hdnnp_ctx* c) {
+    return (c->h_status && (c->h_status[0] & 8) && c->h_status[1] > 0) ? c->h_status[1] - 1 : -1;
+}
+
+}  // namespace hdnnp

@@ -47,6 +47,7 @@ __global__ void k_wrap_bin(Batch b, DevModel m) {
     double x = b.pos[3 * i] - S.org[0], y = b.pos[3 * i + 1] - S.org[1], zz = b.pos[3 * i + 2] - S.org[2];
     if (!isfinite(x) || !isfinite(y) || !isfinite(zz)) {  // device-resident input: flag, keep indices valid
         atomicOr(&b.status[0], 8);
+        atomicMax(&b.status[2], b.sid[i] + 1);  // last structure with such an atom
         x = y = zz = 0.0;
     }
     double s0, s1, s2;

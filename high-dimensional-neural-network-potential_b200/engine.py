@@ -73,6 +73,17 @@ def lib():
     L.hdnnp_last_launch_count.argtypes = [P, C.POINTER(C.c_int)]
     L.hdnnp_ctx_set_profiling.argtypes = [P, C.c_int]
     L.hdnnp_profile_read.argtypes = [P, D, I64, C.c_int]
+    L.hdnnp_server_create.argtypes = [P, P, C.POINTER(C.c_void_p)]
+    L.hdnnp_server_destroy.argtypes = [P]
+    L.hdnnp_server_destroy.restype = None
+    L.hdnnp_server_add_walker.argtypes = [P, C.c_int, I, D, C.c_int, D, D, D, C.POINTER(C.c_int)]
+    L.hdnnp_server_remove_walker.argtypes = [P, C.c_int]
+    L.hdnnp_server_submit.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64,
+                                      C.POINTER(C.c_uint64)]
+    L.hdnnp_server_wait.argtypes = [P, C.c_uint64, C.c_int, D, D, D, D]
+    L.hdnnp_server_next_done.argtypes = [P, C.c_int, C.POINTER(C.c_uint64)]
+    L.hdnnp_server_read_walker.argtypes = [P, C.c_int, D, D]
+    L.hdnnp_server_stats.argtypes = [P, D, D, D, D, C.POINTER(C.c_size_t), C.c_int]
     _lib = L
     return L
 

@@ -170,6 +170,75 @@ int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches);
 int hdnnp_ctx_set_profiling(hdnnp_ctx* c, int on);
 int hdnnp_profile_read(hdnnp_ctx* c, double* stage_ms /* [8] */, int64_t* counters /* [8] */, int reset);
 
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference, which evaluates one structure per call
+ * from a user-written MD loop (src/potentials/hdnnpExample.f90:59-72).
+ * A server keeps many walkers (MD or Monte Carlo trajectories) resident in
+ * device memory -- positions, momenta, masses, last forces and the state
+ * before the last trial move -- and evaluates their requests by continuous
+ * batching: worker threads, each with its own evaluation context and CUDA
+ * stream, take pending requests in arrival order, pack those of idle walkers
+ * into a batch of at most max_batch_atoms atoms and evaluate it with the
+ * batched pipeline; requests that arrive meanwhile join the next batch, and
+ * with workers >= 2 consecutive batches overlap on the GPU.  Requests of one
+ * walker run in submission order.  A walker's result does not depend on
+ * which other walkers share its batch (bitwise for the FP64 form).
+ * Admission: walkers and the workers' workspaces are charged against
+ * hbm_budget; hdnnp_server_add_walker returns HDNNP_E_CAPACITY when a walker
+ * does not fit (remove walkers to admit new ones).                          */
+typedef struct hdnnp_server hdnnp_server;
+
+typedef struct {
+    size_t hbm_budget;   /* bytes for walkers + workspaces; 0 = no limit         */
+    int max_batch_atoms; /* atom slots of one batch (also the largest walker)    */
+    int workers;         /* concurrent batches, 1..8                             */
+    int precision;       /* HDNNP_PREC_FP64 or HDNNP_PREC_MIXED                  */
+} hdnnp_server_opts;
+
+typedef enum {
+    HDNNP_REQ_EVAL = 0,      /* energy, forces, dEdLat of the current positions  */
+    HDNNP_REQ_MC_TRIAL = 1,  /* keep the state, displace every coordinate by
+                                N(0, sigma) (generator keyed by seed and the
+                                walker's step count), then evaluate              */
+    HDNNP_REQ_MC_REJECT = 2, /* restore the state kept by the last trial; no
+                                evaluation and no result besides the status      */
+    HDNNP_REQ_MD_STEP = 3    /* velocity Verlet step of length dt with the last
+                                forces (hdnnpExample.f90:61-64), then evaluate;
+                                needs masses and a previous EVAL                 */
+} hdnnp_request_kind;
+
+int hdnnp_server_create(hdnnp_model* m, const hdnnp_server_opts* opts, hdnnp_server** out);
+/* Stops the workers after their current batch; pending requests are dropped. */
+void hdnnp_server_destroy(hdnnp_server* s);
+
+/* Z[nat], pos[3*nat]; lat[9] is used when periodic != 0.  masses[nat] and
+ * momenta[3*nat] may be NULL (no MD; momenta default to zero).             */
+int hdnnp_server_add_walker(hdnnp_server* s, int nat, const int32_t* Z, const double* pos, int periodic,
+                            const double* lat, const double* masses, const double* momenta, int* walker);
+/* Frees a walker's device memory; HDNNP_E_STATE while it has requests.      */
+int hdnnp_server_remove_walker(hdnnp_server* s, int walker);
+
+int hdnnp_server_submit(hdnnp_server* s, int walker, int kind, double dt, double sigma, uint64_t seed,
+                        uint64_t* ticket);
+/* Waits up to timeout_ms (0 = poll) for a request; HDNNP_E_TIMEOUT if it is
+ * not finished (the ticket stays valid).  On completion the ticket is
+ * consumed and energy, forces[3*nat], dEdLat[9] (zero for molecules) and the
+ * submit-to-completion latency are written where the pointers are non-NULL. */
+int hdnnp_server_wait(hdnnp_server* s, uint64_t ticket, int timeout_ms, double* energy, double* forces,
+                      double* dEdLat, double* latency_ms);
+/* Waits up to timeout_ms for the next finished request not yet reported by
+ * this call (completion order) and returns its ticket, still to be consumed
+ * by hdnnp_server_wait; HDNNP_E_TIMEOUT if none.  Tickets consumed by
+ * hdnnp_server_wait before they are reported are skipped.                    */
+int hdnnp_server_next_done(hdnnp_server* s, int timeout_ms, uint64_t* ticket);
+/* Current positions and momenta of an idle walker (HDNNP_E_STATE if busy).  */
+int hdnnp_server_read_walker(hdnnp_server* s, int walker, double* pos, double* momenta);
+/* Latency percentiles over the finished requests, evaluated atoms per second
+ * between the first submit and the last completion, mean requests per batch,
+ * and HBM bytes charged to walkers + workspaces.  reset != 0 clears them.    */
+int hdnnp_server_stats(hdnnp_server* s, double* p50_ms, double* p99_ms, double* atom_steps_per_s,
+                       double* mean_batch_requests, size_t* hbm_charged, int reset);
+
 #ifdef __cplusplus
 }
 #endif
