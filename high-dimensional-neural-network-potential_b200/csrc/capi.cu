@@ -524,20 +524,26 @@ int collect_profile(hdnnp_ctx* c) {
 // Core pipeline; inputs already on the device in c->Z / c->pos (or external
 // device pointers), structure set-up in c->hinfo.
 int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const double* posd, double* energy_d,
-                 double* force_d, double* dEdLat_d, cudaStream_t st) {
+                 double* force_d, double* dEdLat_d, cudaStream_t st, PipePlan* pp = nullptr) {
     hdnnp_model* m = c->model;
     DevModel D = m->dev;
     // runtime-zeta variant of a compiled-zeta shape (same product layout)
     if (c->runtime_zeta && D.fast == 5) D.fast = 1;
     if (c->runtime_zeta && D.fast == 6) D.fast = 2;
     int ncells = 0;
-    for (auto& S : c->hinfo) {
-        S.cell_off = ncells;
-        ncells += S.ngrid[0] * S.ngrid[1] * S.ngrid[2];
-    }
     int r;
-    if ((r = c->info.ensure(nstruct))) return r;
-    CUDA_TRY(cudaMemcpyAsync(c->info.p, c->hinfo.data(), sizeof(StructInfo) * nstruct, cudaMemcpyHostToDevice, st));
+    if (!pp || pp->upload) {
+        for (auto& S : c->hinfo) {
+            S.cell_off = ncells;
+            // a molecule of a plan gets the largest grid its box may take
+            ncells += (pp && pp->dev_boxes && !S.periodic) ? 64 * S.nat + 4096 : S.ngrid[0] * S.ngrid[1] * S.ngrid[2];
+        }
+        if ((r = c->info.ensure(nstruct))) return r;
+        CUDA_TRY(cudaMemcpyAsync(c->info.p, c->hinfo.data(), sizeof(StructInfo) * nstruct, cudaMemcpyHostToDevice, st));
+        if (pp) pp->ncells = ncells;
+    } else {
+        ncells = pp->ncells;
+    }
     const size_t N = natoms;
     if ((r = c->sid.ensure(N)) || (r = c->elem.ensure(N)) || (r = c->wpos.ensure(3 * N)) || (r = c->cell_of.ensure(N)) ||
         (r = c->cell_cnt.ensure(ncells + 1)) || (r = c->cell_start.ensure(ncells + 1)) ||
@@ -577,8 +583,12 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.force = force_d;
     b.energy = energy_d;
     b.dEdLat = dEdLat_d;
+    b.rc_list = pp ? pp->rc_list : 0.0;
+    b.rebuild = pp ? pp->rebuild : nullptr;
+    b.wshift = pp ? pp->wshift : nullptr;
+    b.pos_ref = pp ? pp->pos_ref : nullptr;
     int L = 0;
-    if (c->profile) {
+    if (c->profile && !pp) {
         if ((r = collect_profile(c))) return r;
         for (auto& e : c->ev)
             if (!e) CUDA_TRY(cudaEventCreate(&e));
@@ -591,29 +601,45 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
         c->host_counts[1] += natoms;
     }
     auto mark = [&](int k) -> int {
-        if (c->profile) CUDA_TRY(cudaEventRecord(c->ev[k], st));
+        if (c->profile && !pp) CUDA_TRY(cudaEventRecord(c->ev[k], st));
         return HDNNP_OK;
     };
     CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
     if ((r = mark(0))) return r;
+    if (pp && pp->dev_boxes) L += launch_molecule_boxes(b, pp->rc_list > 0.0 ? pp->rc_list : D.max_rc, st);
     L += launch_neighbour_build_a(b, D, st);
-    // entry total and the largest count
-    int tot_max[2];
-    CUDA_TRY(cudaMemcpyAsync(c->h_status + 2, b.nei_off + natoms, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(c->h_status + 3, b.status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(c->h_status + 1, b.status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    if ((r = check_status(c))) return r;
-    tot_max[0] = c->h_status[2];
-    tot_max[1] = c->h_status[3];
-    if (tot_max[0] < 0) return fail(HDNNP_E_CAPACITY, "more than 2^31 neighbour entries");
-    const size_t E = (size_t)tot_max[0];
+    size_t E = 0;
+    if (pp && pp->e_cap > 0) {
+        // planned: no host read; overflow of the capacities is flagged on the device
+        L += launch_capacity_guard(b, pp->e_cap, pp->m_cap, st);
+        E = (size_t)pp->e_cap;
+        b.mmax = pp->m_cap;
+    } else {
+        // entry total and the largest count
+        CUDA_TRY(cudaMemcpyAsync(c->h_status + 2, b.nei_off + natoms, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(c->h_status + 3, b.status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(c->h_status + 1, b.status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        if ((r = check_status(c))) return r;
+        if (c->h_status[2] < 0) return fail(HDNNP_E_CAPACITY, "more than 2^31 neighbour entries");
+        E = (size_t)c->h_status[2];
+        b.mmax = c->h_status[3];
+        if (pp) {
+            // probe evaluation of a plan: capacities with headroom
+            const double f = 1.0 + std::max(pp->margin, 0.0);
+            const double ecap = std::ceil((double)E * f) + 1024.0;
+            if (ecap > (double)INT32_MAX) return fail(HDNNP_E_CAPACITY, "planned neighbour entries above 2^31");
+            pp->e_cap = (long long)ecap;
+            pp->m_cap = (((int)std::ceil(b.mmax * f) + 8) + 31) / 32 * 32;
+            E = (size_t)pp->e_cap;
+            b.mmax = pp->m_cap;
+        }
+    }
     if ((r = c->nei_j.ensure(E + 1)) || (r = c->nei_s.ensure(E + 1)) || (r = c->nei_rev.ensure(E + 1)) ||
         (r = c->gent.ensure(3 * E + 3)))
         return r;
     b.nentries = (int)E;
-    b.mmax = tot_max[1];
     b.nei_j = c->nei_j.p;
     b.nei_s = c->nei_s.p;
     b.nei_rev = c->nei_rev.p;
@@ -1124,6 +1150,39 @@ int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* 
 // Device error flags of the last evaluation on c (valid after its stream has
 // been synchronised).
 int ctx_check_status(hdnnp_ctx* c) { return check_status(c); }
+
+// Host set-up of a resident plan: periodic structures as struct_setup with
+// the list cutoff; molecules get their box on the device every evaluation.
+int ctx_plan_setup(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* periodic, const double* lat,
+                   double rc_list) {
+    c->hinfo.resize(nstruct);
+    if (off[0] != 0) return fail(HDNNP_E_INPUT, "atom_off[0] must be 0");
+    for (int s = 0; s < nstruct; ++s) {
+        const int64_t a0 = off[s], a1 = off[s + 1];
+        if (a1 <= a0) return fail(HDNNP_E_INPUT, "structure " + std::to_string(s) + " has no atoms");
+        if (a1 > INT32_MAX) return fail(HDNNP_E_CAPACITY, "more than 2^31 atoms");
+        StructInfo& S = c->hinfo[s];
+        if (periodic[s]) {
+            int r = struct_setup((int)(a1 - a0), nullptr, 1, lat + 9 * s, rc_list, S);
+            if (r) return fail(r, "structure " + std::to_string(s) + ": " + g_err);
+        } else {
+            std::memset(&S, 0, sizeof S);
+            S.ngrid[0] = S.ngrid[1] = S.ngrid[2] = 1;
+        }
+        S.atom_off = (int)a0;
+        S.nat = (int)(a1 - a0);
+    }
+    return HDNNP_OK;
+}
+
+int ctx_run_planned(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Z_dev, const double* pos_dev,
+                    double* energy_dev, double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan& pp) {
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    return run_pipeline(c, nstruct, natoms, Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st, &pp);
+}
+
+// Device error flags of c's evaluations ([4] ints, flags in [0]).
+int* ctx_status_dev(hdnnp_ctx* c) { return c->status.p; }
 
 // Batch index of a structure with a non-finite position in the last
 // evaluation on c, or -1.

@@ -152,6 +152,35 @@ struct Batch {
     float* gentf;
     float* gselff;
     float* virf;
+    // Resident plans (plan.cu).  rc_list: neighbour-list cutoff (0: the
+    // potential's max_rc; max_rc + skin for Verlet-skin lists, whose entries
+    // beyond rc the symmetry-function kernels drop).  rebuild: device flag,
+    // null = build every evaluation; when it is 0 the list, cells and wrap
+    // translations of the last build are kept and positions are translated
+    // by wshift instead of wrapped.  wshift[3*natoms]: wrapped - raw position
+    // of each atom at the last build; pos_ref[3*natoms]: raw positions at the
+    // last build.
+    double rc_list;
+    const int* rebuild;
+    double* wshift;
+    double* pos_ref;
+};
+
+// Resident-plan mode of the pipeline (plan.cu): capacities fixed in advance
+// so that an evaluation needs no host read and can be captured in a CUDA
+// graph.  e_cap == 0 on the first (probe) evaluation: the pipeline reads the
+// counts, sets e_cap / m_cap with `margin` headroom and sizes the workspace.
+struct PipePlan {
+    long long e_cap = 0;     // neighbour entries
+    int m_cap = 0;           // largest per-atom count (multiple of 32)
+    double margin = 0.25;
+    int ncells = 0;          // cells reserved (molecules: the largest grid allowed)
+    bool upload = true;      // host set-up -> device (false inside a capture)
+    bool dev_boxes = false;  // molecules: boxes recomputed on the device
+    double rc_list = 0.0;    // neighbour-list cutoff (max_rc + skin)
+    int* rebuild = nullptr;  // Verlet-skin flag (null: rebuild every time)
+    double* wshift = nullptr;
+    double* pos_ref = nullptr;
 };
 
 // packed image shift: three signed 8-bit lattice multiples
@@ -169,6 +198,11 @@ __host__ __device__ inline void unpack_shift(int p, int& x, int& y, int& z) {
 int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s);  // wrap, bin, count
 int launch_scan(int* data, int n, int* tmp, int* total_out_dev, cudaStream_t s);   // exclusive scan in place, total in data[n]
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s);  // fill + reverse
+// Planned evaluations (no host read between the count and the fill pass):
+// flag 32 and empty lists when the entries or the largest count exceed the
+// capacities; molecules' boxes and grids recomputed on the device.
+int launch_capacity_guard(const Batch& b, long long e_cap, int m_cap, cudaStream_t s);
+int launch_molecule_boxes(const Batch& b, double rc, cudaStream_t s);
 int launch_sf_values(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_sf_gradients(const Batch& b, const DevModel& m, cudaStream_t s);

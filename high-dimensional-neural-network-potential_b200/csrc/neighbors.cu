@@ -12,7 +12,9 @@
 // symmetry-function kernels treat it implicitly.
 //
 // HBM-bound integer/FP64 work: one thread per atom (wrap, count, fill, force
-// gather), one thread per entry (reverse index), one thread per cell (sort).
+// gather), one warp per atom (reverse index), one thread per cell (sort).
+#include <cmath>
+
 #include "engine.h"
 
 namespace hdnnp {
@@ -28,6 +30,9 @@ __device__ __forceinline__ void matvec(const double* a, double x, double y, doub
     oz = a[2] * x + a[5] * y + a[8] * z;
 }
 
+// Verlet-skin reuse: the list of the last build stays valid this evaluation.
+__device__ __forceinline__ bool keep_list(const Batch& b) { return b.rebuild && !*b.rebuild; }
+
 __global__ void k_atom_struct(const StructInfo* info, int nstruct, int* sid) {
     int s = blockIdx.x;
     if (s >= nstruct) return;
@@ -39,6 +44,18 @@ __global__ void k_atom_struct(const StructInfo* info, int nstruct, int* sid) {
 __global__ void k_wrap_bin(Batch b, DevModel m) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= b.natoms) return;
+    if (keep_list(b)) {
+        // same translation as at the last build: distances to the listed images stay consistent
+        for (int d = 0; d < 3; ++d) {
+            const double x = b.pos[3 * i + d];
+            if (!isfinite(x)) {
+                atomicOr(&b.status[0], 8);
+                atomicMax(&b.status[2], b.sid[i] + 1);
+            }
+            b.wpos[3 * i + d] = isfinite(x) ? x + b.wshift[3 * i + d] : b.pos_ref[3 * i + d] + b.wshift[3 * i + d];
+        }
+        return;
+    }
     const StructInfo& S = b.info[b.sid[i]];
     int z = b.Z[i];
     int e = (z >= 1 && z <= 118) ? m.z2e[z] : -1;
@@ -60,6 +77,14 @@ __global__ void k_wrap_bin(Batch b, DevModel m) {
     b.wpos[3 * i] = wx;
     b.wpos[3 * i + 1] = wy;
     b.wpos[3 * i + 2] = wz;
+    if (b.wshift) {
+        b.wshift[3 * i] = wx - b.pos[3 * i];
+        b.wshift[3 * i + 1] = wy - b.pos[3 * i + 1];
+        b.wshift[3 * i + 2] = wz - b.pos[3 * i + 2];
+        b.pos_ref[3 * i] = b.pos[3 * i];
+        b.pos_ref[3 * i + 1] = b.pos[3 * i + 1];
+        b.pos_ref[3 * i + 2] = b.pos[3 * i + 2];
+    }
     // cell from the fractional coordinates of the wrapped position
     double f0, f1, f2;
     matvec(S.hinv, wx, wy, wz, f0, f1, f2);
@@ -73,7 +98,7 @@ __global__ void k_wrap_bin(Batch b, DevModel m) {
 
 __global__ void k_fill_cells(Batch b, int* cursor) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b.natoms) return;
+    if (i >= b.natoms || keep_list(b)) return;
     int c = b.cell_of[i];
     int p = atomicAdd(&cursor[c], 1);
     b.cell_atoms[b.cell_start[c] + p] = i;
@@ -82,7 +107,7 @@ __global__ void k_fill_cells(Batch b, int* cursor) {
 // deterministic order inside a cell: increasing atom index
 __global__ void k_sort_cells(Batch b) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= b.ncells) return;
+    if (c >= b.ncells || keep_list(b)) return;
     int s = b.cell_start[c], e = b.cell_start[c + 1];
     for (int p = s + 1; p < e; ++p) {
         int v = b.cell_atoms[p];
@@ -99,9 +124,10 @@ __global__ void k_sort_cells(Batch b) {
 template <bool kFill>
 __global__ void k_neighbours(Batch b, DevModel m) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= b.natoms) return;
+    if (i >= b.natoms || keep_list(b)) return;
+    if (kFill && b.status[3]) return;  // planned capacity exceeded: the lists stay empty
     const StructInfo& S = b.info[b.sid[i]];
-    const double rc = m.max_rc, rc2 = rc * rc;
+    const double rc = b.rc_list > 0.0 ? b.rc_list : m.max_rc, rc2 = rc * rc;
     const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
     const int c = b.cell_of[i] - S.cell_off;
     const int ix = c / (S.ngrid[1] * S.ngrid[2]);
@@ -159,24 +185,34 @@ __global__ void k_neighbours(Batch b, DevModel m) {
     if (!kFill) b.nei_cnt[i] = n;
 }
 
-// reverse entry: entry e = (a -> j, S) maps to the entry (j -> a, -S)
+// Reverse-entry index: for entry e = (a -> j, shift s) the entry (j -> a, -s)
+// of j's list.  One warp per atom a; for each of a's entries the 32 lanes scan
+// j's list in coalesced 32-entry chunks and the ballot picks the first match.
 __global__ void k_reverse(Batch b) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= b.natoms) return;
-    for (int e = b.nei_off[a]; e < b.nei_off[a + 1]; ++e) {
+    const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= b.natoms || keep_list(b)) return;  // uniform per warp
+    const int e1 = b.nei_off[a + 1];
+    for (int e = b.nei_off[a]; e < e1; ++e) {
         const int j = b.nei_j[e];
         int sx, sy, sz;
         unpack_shift(b.nei_s[e], sx, sy, sz);
         const int want = pack_shift(-sx, -sy, -sz);
+        const int f1 = b.nei_off[j + 1];
         int r = -1;
-        for (int f = b.nei_off[j]; f < b.nei_off[j + 1]; ++f) {
-            if (b.nei_j[f] == a && b.nei_s[f] == want) {
-                r = f;
+        for (int fb = b.nei_off[j]; fb < f1; fb += 32) {
+            const int f = fb + lane;
+            const bool hit = f < f1 && b.nei_j[f] == a && b.nei_s[f] == want;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+                r = fb + __ffs(m) - 1;
                 break;
             }
         }
-        if (r < 0) atomicOr(&b.status[0], 2);  // asymmetric list (should not happen)
-        b.nei_rev[e] = r < 0 ? e : r;
+        if (lane == 0) {
+            if (r < 0) atomicOr(&b.status[0], 2);  // asymmetric list (should not happen)
+            b.nei_rev[e] = r < 0 ? e : r;
+        }
     }
 }
 
@@ -274,8 +310,169 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s) 
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) {
     const int gA = (b.natoms + kThreads - 1) / kThreads;
     k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
-    k_reverse<<<gA, kThreads, 0, s>>>(b);
+    const long long warps_threads = 32LL * b.natoms;
+    k_reverse<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     return 2;
+}
+
+// ---------------------------------------------------------------- planned capacities
+namespace {
+
+// After the count pass of an evaluation without a host read: entries or the
+// largest per-atom count above the planned capacity set flag 32 and status[3],
+// and the lists are emptied so that no later kernel indexes past its arrays.
+__global__ void k_caps_check(Batch b, long long e_cap, int m_cap) {
+    if (blockIdx.x || threadIdx.x) return;
+    const int total = b.nei_off[b.natoms];
+    if (total < 0 || (long long)total > e_cap || b.status[1] > m_cap) {
+        atomicOr(&b.status[0], 32);
+        b.status[3] = 1;
+    }
+}
+
+__global__ void k_caps_clear(Batch b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= b.natoms && b.status[3]) b.nei_off[i] = 0;
+}
+
+// Device copies of the host set-up arithmetic (struct_setup, n_cells and inv3
+// in capi.cu) with every operation rounded on its own (no contraction), so the
+// device-built box of a molecule equals the host-built one bit for bit.
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dv(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ void d_cross(const double* a, const double* b, double* c) {
+    c[0] = sub(mul(a[1], b[2]), mul(a[2], b[1]));
+    c[1] = sub(mul(a[2], b[0]), mul(a[0], b[2]));
+    c[2] = sub(mul(a[0], b[1]), mul(a[1], b[0]));
+}
+
+__device__ void d_n_cells(const double* lat, double cut, int* n) {
+    double axb[3], axc[3], bxc[3];
+    d_cross(lat, lat + 3, axb);
+    d_cross(lat, lat + 6, axc);
+    d_cross(lat + 3, lat + 6, bxc);
+    double* vs[3] = {axb, axc, bxc};
+    for (double* v : vs) {
+        const double s = __dsqrt_rn(add(add(mul(v[0], v[0]), mul(v[1], v[1])), mul(v[2], v[2])));
+        for (int k = 0; k < 3; ++k) v[k] = dv(v[k], s);
+    }
+    const double p0 = add(add(mul(lat[0], bxc[0]), mul(lat[1], bxc[1])), mul(lat[2], bxc[2]));
+    const double p1 = add(add(mul(lat[3], axc[0]), mul(lat[4], axc[1])), mul(lat[5], axc[2]));
+    const double p2 = add(add(mul(lat[6], axb[0]), mul(lat[7], axb[1])), mul(lat[8], axb[2]));
+    n[0] = (int)ceil(dv(cut, fabs(p0)));
+    n[1] = (int)ceil(dv(cut, fabs(p1)));
+    n[2] = (int)ceil(dv(cut, fabs(p2)));
+}
+
+__device__ void d_inv3(const double* a, double* b) {
+    auto A = [&](int r, int c) { return a[r + 3 * c]; };
+    const double d = sub(sub(sub(add(add(mul(mul(a[0], a[4]), a[8]), mul(mul(a[3], a[7]), a[2])),
+                                     mul(mul(a[6], a[1]), a[5])),
+                                 mul(mul(a[0], a[7]), a[5])),
+                             mul(mul(a[3], a[1]), a[8])),
+                         mul(mul(a[6], a[4]), a[2]));
+    const double r0[3] = {A(0, 0), A(0, 1), A(0, 2)}, r1[3] = {A(1, 0), A(1, 1), A(1, 2)},
+                 r2[3] = {A(2, 0), A(2, 1), A(2, 2)};
+    const double c0[3] = {sub(mul(r1[1], r2[2]), mul(r1[2], r2[1])), sub(mul(r0[2], r2[1]), mul(r0[1], r2[2])),
+                          sub(mul(r0[1], r1[2]), mul(r0[2], r1[1]))};
+    const double c1[3] = {sub(mul(r1[2], r2[0]), mul(r1[0], r2[2])), sub(mul(r0[0], r2[2]), mul(r0[2], r2[0])),
+                          sub(mul(r0[2], r1[0]), mul(r0[0], r1[2]))};
+    const double c2[3] = {sub(mul(r1[0], r2[1]), mul(r1[1], r2[0])), sub(mul(r0[1], r2[0]), mul(r0[0], r2[1])),
+                          sub(mul(r0[0], r1[1]), mul(r0[1], r1[0]))};
+    for (int k = 0; k < 3; ++k) {
+        b[0 + 3 * k] = dv(c0[k], d);
+        b[1 + 3 * k] = dv(c1[k], d);
+        b[2 + 3 * k] = dv(c2[k], d);
+    }
+}
+
+// Artificial box of each molecule from its current positions (the reference's
+// non-periodic branch, neighborLists.f90:129-169): origin min - 1e-4, edge
+// extent + 1e-4, grid of >= 0.6 rc cells coarsened like the host set-up, and
+// the search range.  One block per structure; periodic structures keep their
+// set-up.  Cells were reserved for the largest grid the coarsening allows.
+__global__ void k_molecule_boxes(Batch b, double rc) {
+    StructInfo& S = const_cast<StructInfo*>(b.info)[blockIdx.x];
+    if (S.periodic || keep_list(b)) return;
+    __shared__ double red[6][32];
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const double* p = b.pos + 3 * (size_t)S.atom_off;
+    for (int i = threadIdx.x; i < S.nat; i += blockDim.x)
+        for (int d = 0; d < 3; ++d) {
+            mn[d] = fmin(mn[d], p[3 * i + d]);
+            mx[d] = fmax(mx[d], p[3 * i + d]);
+        }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int d = 0; d < 3; ++d)
+        for (int o = 16; o; o >>= 1) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) {
+            red[d][w] = mn[d];
+            red[3 + d][w] = mx[d];
+        }
+    __syncthreads();
+    if (threadIdx.x) return;
+    for (int k = 1; k < nw; ++k)
+        for (int d = 0; d < 3; ++d) {
+            red[d][0] = fmin(red[d][0], red[d][k]);
+            red[3 + d][0] = fmax(red[3 + d][0], red[3 + d][k]);
+        }
+    if (!(isfinite(red[0][0]) && isfinite(red[1][0]) && isfinite(red[2][0]) && isfinite(red[3][0]) &&
+          isfinite(red[4][0]) && isfinite(red[5][0]))) {
+        // non-finite positions: keep the previous box; the wrap kernel flags the atoms
+        return;
+    }
+    for (int k = 0; k < 9; ++k) S.h[k] = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        S.org[d] = sub(red[d][0], 1.e-4);
+        // max(x - org) = max(x) - org: subtraction by a constant is monotone
+        S.h[d + 3 * d] = add(sub(red[3 + d][0], S.org[d]), 1.e-4);
+    }
+    d_inv3(S.h, S.hinv);
+    const double target = mul(rc, 0.6);
+    long long ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+        const double len = __dsqrt_rn(add(add(mul(S.h[3 * d], S.h[3 * d]), mul(S.h[3 * d + 1], S.h[3 * d + 1])),
+                                          mul(S.h[3 * d + 2], S.h[3 * d + 2])));
+        S.ngrid[d] = (int)dv(len, target) + 1;
+        ncell *= S.ngrid[d];
+    }
+    const long long limit = 64LL * S.nat + 4096;
+    while (ncell > limit) {
+        ncell = 1;
+        for (int d = 0; d < 3; ++d) {
+            S.ngrid[d] = max(1, S.ngrid[d] / 2);
+            ncell *= S.ngrid[d];
+        }
+    }
+    double grid[9];
+    for (int d = 0; d < 3; ++d)
+        for (int r = 0; r < 3; ++r) grid[r + 3 * d] = dv(S.h[r + 3 * d], (double)S.ngrid[d]);
+    d_n_cells(grid, rc, S.nsearch);
+    for (int d = 0; d < 3; ++d)
+        if (S.nsearch[d] > 64) {
+            atomicOr(&b.status[0], 32);  // reported as a capacity error
+            S.nsearch[d] = 64;
+        }
+}
+
+}  // namespace
+
+int launch_capacity_guard(const Batch& b, long long e_cap, int m_cap, cudaStream_t s) {
+    k_caps_check<<<1, 32, 0, s>>>(b, e_cap, m_cap);
+    k_caps_clear<<<(b.natoms + 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(b);
+    return 2;
+}
+
+int launch_molecule_boxes(const Batch& b, double rc, cudaStream_t s) {
+    k_molecule_boxes<<<b.nstruct, 128, 0, s>>>(b, rc);
+    return 1;
 }
 
 }  // namespace hdnnp

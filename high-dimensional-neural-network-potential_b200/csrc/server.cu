@@ -39,6 +39,7 @@
 
 #include "../../include/hdnnp_gpu.h"
 #include "engine.h"
+#include "integrate.cuh"
 
 namespace hdnnp {
 int model_device(const hdnnp_model* m);
@@ -56,59 +57,6 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr int kThreads = 256;
-
-// ------------------------------------------------------------------ device steps
-// SplitMix64 finaliser (Steele, Lea, Flood, OOPSLA 2014): counter-based draws.
-__device__ __host__ __forceinline__ unsigned long long mix64(unsigned long long x) {
-    x += 0x9E3779B97F4A7C15ull;
-    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-    return x ^ (x >> 31);
-}
-
-// Trial move: keep pos and force, pos += sigma * N(0,1) per coordinate
-// (Box-Muller transform of two 53-bit uniforms drawn from (key, coordinate)).
-__global__ void k_mc_trial(double* __restrict__ pos, double* __restrict__ pos_keep, const double* __restrict__ force,
-                           double* __restrict__ force_keep, int n3, double sigma, unsigned long long key) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n3) return;
-    const double x = pos[i];
-    pos_keep[i] = x;
-    force_keep[i] = force[i];
-    const unsigned long long a = mix64(key + 2ull * (unsigned long long)i);
-    const unsigned long long b = mix64(key + 2ull * (unsigned long long)i + 1ull);
-    const double u1 = ((double)(a >> 11) + 1.0) * (1.0 / 9007199254740992.0);  // (0, 1]
-    const double u2 = (double)(b >> 11) * (1.0 / 9007199254740992.0);          // [0, 1)
-    pos[i] = x + sigma * sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-}
-
-__global__ void k_mc_reject(double* __restrict__ pos, const double* __restrict__ pos_keep, double* __restrict__ force,
-                            const double* __restrict__ force_keep, int n3) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n3) return;
-    pos[i] = pos_keep[i];
-    force[i] = force_keep[i];
-}
-
-// Velocity Verlet, first half (hdnnpExample.f90:61-62):
-// x += p/m dt + F/(2m) dt^2, keep F as the previous forces.
-__global__ void k_md_drift(double* __restrict__ pos, const double* __restrict__ mom, const double* __restrict__ mass,
-                           const double* __restrict__ force, double* __restrict__ force_prev, int n3, double dt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n3) return;
-    const double m = mass[i / 3];
-    pos[i] += mom[i] / m * dt + 0.5 * force[i] / m * dt * dt;
-    force_prev[i] = force[i];
-}
-
-// Second half (hdnnpExample.f90:64): p += dt/2 (F_new + F_prev), F = F_new.
-__global__ void k_md_kick(double* __restrict__ mom, const double* __restrict__ f_new,
-                          const double* __restrict__ force_prev, double* __restrict__ force, int n3, double dt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n3) return;
-    mom[i] += 0.5 * dt * (f_new[i] + force_prev[i]);
-    force[i] = f_new[i];
-}
 
 inline int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 

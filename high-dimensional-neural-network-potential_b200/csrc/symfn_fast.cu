@@ -121,20 +121,52 @@ template <> struct Buf<float> {
     static __device__ float* vir(const Batch& b) { return b.virf; }
 };
 
+// Relative vector centre - image of neighbour entry (j, packed shift), FP64.
+__device__ __forceinline__ void entry_vec(const Batch& b, const StructInfo& S, double xi, double yi, double zi, int j,
+                                          int sh, double& dx, double& dy, double& dz) {
+    int sx, sy, sz;
+    unpack_shift(sh, sx, sy, sz);
+    const double* h = S.h;
+    double lx = 0, ly = 0, lz = 0;
+    if (sz) { lx += h[6] * sz; ly += h[7] * sz; lz += h[8] * sz; }
+    if (sy) { lx += h[3] * sy; ly += h[4] * sy; lz += h[5] * sy; }
+    if (sx) { lx += h[0] * sx; ly += h[1] * sx; lz += h[2] * sx; }
+    dx = xi - (b.wpos[3 * j] + lx);
+    dy = yi - (b.wpos[3 * j + 1] + ly);
+    dz = zi - (b.wpos[3 * j + 2] + lz);
+}
+
 // Stage the neighbour entries of atom i sorted by element (stable).  The
 // relative vectors are formed in FP64 from the wrapped positions and image
-// shifts and then rounded to T.
+// shifts and then rounded to T.  With a Verlet-skin list (list cutoff above
+// rc) only entries with r < rc are staged; the gradient pass writes zero
+// gradients for the others.  Returns the number of staged entries.
 template <typename T, bool kGrad>
-__device__ void fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>& s, int lane, int M) {
+__device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>& s, int lane, int M) {
     const int e0 = b.nei_off[i];
     const int nel = m.nel;
+    const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
+    const StructInfo& S = b.info[b.sid[i]];
+    const double rc = m.rc[c];
+    const bool filt = b.rc_list > rc;
+    const double rc2 = rc * rc;
     if (lane < nel) s.cur[lane] = 0;
     __syncwarp();
     for (int base = 0; base < M; base += 32) {
         const int q = base + lane;
-        const unsigned act = __ballot_sync(kFull, q < M);
-        if (q < M) {
-            const int el = b.elem[b.nei_j[e0 + q]];
+        bool keep = q < M;
+        int el = 0;
+        if (keep) {
+            const int j = b.nei_j[e0 + q];
+            el = b.elem[j];
+            if (filt) {
+                double dx, dy, dz;
+                entry_vec(b, S, xi, yi, zi, j, b.nei_s[e0 + q], dx, dy, dz);
+                keep = dx * dx + dy * dy + dz * dz < rc2;
+            }
+        }
+        const unsigned act = __ballot_sync(kFull, keep);
+        if (keep) {
             const unsigned peers = __match_any_sync(act, el);
             if ((peers & lanemask_lt()) == 0) s.cur[el] += __popc(peers);
         }
@@ -151,33 +183,36 @@ __device__ void fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>
     __syncwarp();
     if (lane < nel) s.cur[lane] = s.est[lane];
     __syncwarp();
-    const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
-    const StructInfo& S = b.info[b.sid[i]];
-    const double rc = m.rc[c];
     for (int base = 0; base < M; base += 32) {
         const int q = base + lane;
-        const unsigned act = __ballot_sync(kFull, q < M);
         int slot = 0, el = 0, j = 0, sh = 0;
-        if (q < M) {
+        double dx = 0, dy = 0, dz = 0;
+        bool keep = q < M;
+        if (keep) {
             j = b.nei_j[e0 + q];
             sh = b.nei_s[e0 + q];
             el = b.elem[j];
+            entry_vec(b, S, xi, yi, zi, j, sh, dx, dy, dz);
+            if (filt && !(dx * dx + dy * dy + dz * dz < rc2)) {
+                keep = false;
+                if (kGrad) {
+                    T* gent = Buf<T>::gent(b);
+                    const size_t e = (size_t)(e0 + q);
+                    gent[3 * e] = (T)0;
+                    gent[3 * e + 1] = (T)0;
+                    gent[3 * e + 2] = (T)0;
+                }
+            }
+        }
+        const unsigned act = __ballot_sync(kFull, keep);
+        if (keep) {
             const unsigned peers = __match_any_sync(act, el);
             slot = s.cur[el] + __popc(peers & lanemask_lt());
             __syncwarp(act);
             if ((peers & lanemask_lt()) == 0) s.cur[el] += __popc(peers);
         }
         __syncwarp();
-        if (q < M) {
-            int sx, sy, sz;
-            unpack_shift(sh, sx, sy, sz);
-            const double* h = S.h;
-            double lx = 0, ly = 0, lz = 0;
-            if (sz) { lx += h[6] * sz; ly += h[7] * sz; lz += h[8] * sz; }
-            if (sy) { lx += h[3] * sy; ly += h[4] * sy; lz += h[5] * sy; }
-            if (sx) { lx += h[0] * sx; ly += h[1] * sx; lz += h[2] * sx; }
-            const double dx = xi - (b.wpos[3 * j] + lx), dy = yi - (b.wpos[3 * j + 1] + ly),
-                         dz = zi - (b.wpos[3 * j + 2] + lz);
+        if (keep) {
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
             double fc = 0.0, dfc = 0.0;
             if (r < rc) {
@@ -196,6 +231,7 @@ __device__ void fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>
         }
     }
     __syncwarp();
+    return s.est[nel];
 }
 
 // Candidate c of block (a,b) -> slots (j,k) without divisions: rectangular
@@ -345,7 +381,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
             if (lane == 0) atomicOr(&b.status[0], 4);
             continue;
         }
-        fstage<T, false>(b, m, i, c, s, lane, M);
+        const int Ms = fstage<T, false>(b, m, i, c, s, lane, M);
         const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
         const double rc2d = m.rc[c] * m.rc[c];
         T* Gi = Gout + (size_t)i * m.nsf_max;
@@ -491,7 +527,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
             if (lane == 0) atomicOr(&b.status[0], 4);
             continue;
         }
-        fstage<T, true>(b, m, i, c, s, lane, M);
+        const int Ms = fstage<T, true>(b, m, i, c, s, lane, M);
         const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
         const double rc2d = m.rc[c] * m.rc[c];
         const int nsf = m.nsf[c];
@@ -513,7 +549,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
         __syncwarp();
 
         // radial: lane = neighbour slot
-        for (int t = lane; t < M; t += 32) {
+        for (int t = lane; t < Ms; t += 32) {
             const int el = s.el[t];
             const int f0 = m.g2_off[c * nel + el], f1 = m.g2_off[c * nel + el + 1];
             const V4<T> d = s.nb[t];
@@ -640,7 +676,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
         T* gent = Buf<T>::gent(b);
         T sx = 0, sy = 0, sz = 0;
         T v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int t = lane; t < M; t += 32) {
+        for (int t = lane; t < Ms; t += 32) {
             const V4<T> g = s.g[t];
             const V4<T> d = s.nb[t];
             const size_t e = (size_t)s.ent[t];

@@ -170,6 +170,46 @@ int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches);
 int hdnnp_ctx_set_profiling(hdnnp_ctx* c, int on);
 int hdnnp_profile_read(hdnnp_ctx* c, double* stage_ms /* [8] */, int64_t* counters /* [8] */, int reset);
 
+/* ---------------------------------------------------------------- resident plans
+ * No counterpart in the reference, which repeats every set-up step and
+ * rebuilds the neighbour lists on each hdnnpEnergyAndForces call
+ * (hdnnps.f90:333-371).  A plan fixes a batch (atom_off, periodic, lat as for
+ * hdnnp_eval_batch; Z, positions and results in device memory) and captures
+ * one evaluation -- or, with momenta, `steps_per_launch` velocity-Verlet steps
+ * (hdnnpExample.f90:61-64) -- into a CUDA graph; hdnnp_plan_launch replays it
+ * with no host work.  Positions may be changed in place between launches
+ * (lattices and atom counts may not).  Molecules get their bounding box on
+ * the device.  skin > 0: Verlet-skin lists with cutoff max_rc + skin, rebuilt
+ * on the device when an atom has moved more than skin/2 since the last build.
+ * Creating a plan runs one evaluation (results valid afterwards; the MD
+ * steps start from its forces) and reserves neighbour capacity with
+ * `margin` headroom; a later launch that needs more flags it and
+ * hdnnp_plan_sync returns HDNNP_E_CAPACITY (results of that launch are not
+ * valid; create the plan again).  The plan owns a private workspace.       */
+typedef struct hdnnp_plan hdnnp_plan;
+
+typedef struct {
+    int precision;           /* HDNNP_PREC_FP64 or HDNNP_PREC_MIXED                     */
+    double margin;           /* capacity headroom, e.g. 0.25                            */
+    double skin;             /* Verlet skin in Bohr; 0 = rebuild every evaluation      */
+    double* momenta_dev;     /* NULL: evaluation plan; else MD plan (3*natoms doubles) */
+    const double* masses_dev;/* natoms doubles (MD)                                    */
+    double dt;               /* MD time step                                           */
+    int steps_per_launch;    /* MD steps per launch                                    */
+    double* energy_hist_dev; /* NULL or steps_per_launch*nstruct energies per launch    */
+} hdnnp_plan_opts;
+
+int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* opts, int nstruct, const int64_t* atom_off,
+                      const int32_t* periodic, const double* lat, const int32_t* Z_dev, double* pos_dev,
+                      double* energy_dev, double* force_dev, double* dEdLat_dev, hdnnp_plan** out);
+/* Asynchronous on `stream` (NULL: the plan's own stream). */
+int hdnnp_plan_launch(hdnnp_plan* p, void* stream);
+/* Waits for `stream` and returns the device status of the launches since the
+ * last sync; list_builds (may be NULL) = neighbour-list builds among them.  */
+int hdnnp_plan_sync(hdnnp_plan* p, void* stream, int64_t* list_builds);
+int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_per_launch);
+void hdnnp_plan_free(hdnnp_plan* p);
+
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference, which evaluates one structure per call
  * from a user-written MD loop (src/potentials/hdnnpExample.f90:59-72).
