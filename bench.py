@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 import __graft_entry__  # noqa: E402
 
 POT_DIR = os.path.join(ROOT, "tests", "golden", "abx3")
+EXAMPLE_DIR = os.path.join(ROOT, "tests", "golden", "example")
 METRIC = "atom-steps/s (E+F+stress)"
 # MD time step of the served walkers (a.u.).  The random-init potential is
 # stiff: velocity Verlet at the example's 20 a.u. heats its trajectories until
@@ -58,6 +59,7 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=512, help="structures timed through the plain per-structure API")
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="seconds per load point of the serving leg (0: skip)")
+    ap.add_argument("--md", type=int, default=1, help="1: run the device-resident MD legs")
     ap.add_argument("--lean", action="store_true",
                     help="device-resident steps only (no e2e, comparisons, peaks or CPU baseline): for profiler runs")
     return ap.parse_args()
@@ -246,6 +248,69 @@ def serve_leg(pkg, engine, pot, prec, seconds):
             "saturation": sat, "poisson_sweep": sweep}
 
 
+def md_legs(pkg, engine, PLm, pot, torch):
+    """Device-resident MD, one CUDA graph per launch (resident plans).
+
+    methylammonium: the reference's example (8 atoms, non-periodic, example
+      potential, FP64), velocity Verlet at dt = 20 a.u. from seeded 140 K
+      momenta: 1000 steps as 10 launches of a 100-step graph; per-step
+      latency.  Beside it the same MD through the plain per-call API (host
+      integrator, hdnnp_energy_and_forces every step), as the reference runs it.
+    strained_49152: 16x16x16 supercell of the ABX3 cell with a 3 % random
+      triclinic strain (seed 2), Maxwell-Boltzmann 300 K (seed 3), 200 steps
+      as 10 launches of 20, 1 Bohr Verlet skin, mixed precision, dt DT_SYNTH.
+    """
+    W = pkg.workloads
+    out = {}
+
+    def timed(plan, launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        builds = 0
+        e0.record()
+        for _ in range(launches):
+            plan.launch(torch.cuda.current_stream().cuda_stream)
+        e1.record()
+        builds += plan.sync(torch.cuda.current_stream().cuda_stream)
+        return e0.elapsed_time(e1) / 1e3, builds
+
+    s, m, p0 = W.config_c1(EXAMPLE_DIR)
+    pot1 = engine.Hdnnp.from_runner(EXAMPLE_DIR)
+    pl = PLm.Plan(pot1, [s], masses=m, momenta=p0, dt=20.0, steps_per_launch=100, want_dEdLat=False)
+    timed(pl, 1)  # warm-up
+    sec, _ = timed(pl, 10)
+    ats = engine.AtStruct(s["Z"], s["pos"])
+    E, F, _ = pot1.energy_and_forces(ats)
+    x, p = s["pos"].copy(), p0.copy()
+    nh = 200
+    t0 = time.perf_counter()
+    for _ in range(nh):
+        x = x + p / m[:, None] * 20.0 + 0.5 * F / m[:, None] * 400.0
+        Fl = F
+        E, F, _ = pot1.energy_and_forces(engine.AtStruct(s["Z"], x))
+        p = p + 10.0 * (F + Fl)
+    hsec = time.perf_counter() - t0
+    out["methylammonium_md"] = {
+        "workload": "reference example MD: 8 atoms, FP64, dt 20 a.u., 1000 steps (10 graph launches of 100)",
+        "steps_per_s": 1000 / sec, "us_per_step": sec / 1000 * 1e6, "kernels_per_step": pl.info()["kernels_per_launch"] / 100,
+        "plain_api_steps_per_s": nh / hsec, "plain_api_us_per_step": hsec / nh * 1e6}
+    pl.close()
+    pot1.close()
+
+    s3 = W.config_c3()
+    m3, p3 = W.maxwell_boltzmann(s3["Z"], 300.0, 3)
+    pl3 = PLm.Plan(pot, [s3], precision=engine.HDNNP_PREC_MIXED, skin=1.0, masses=m3, momenta=p3, dt=DT_SYNTH,
+                   steps_per_launch=20, want_dEdLat=False)
+    timed(pl3, 1)
+    sec, builds = timed(pl3, 10)
+    nat = len(s3["Z"])
+    out["strained_49152_md"] = {
+        "workload": f"{nat} atoms, 3% triclinic strain, 300 K, 200 MD steps (10 graph launches of 20), "
+                    f"1 Bohr Verlet skin, mixed precision, dt {DT_SYNTH} a.u.",
+        "atom_steps_per_s": nat * 200 / sec, "ms_per_step": sec / 200 * 1e3, "list_builds": builds}
+    pl3.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -282,12 +347,21 @@ def main():
     Ld = torch.zeros(nstruct, 9, dtype=torch.float64, device="cuda")
     stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream is NULL)
 
-    def step_device():
+    def step_eager():
+        # hdnnp_eval_batch_device: host set-up and one host read of the entry total per step
         engine._check(L.hdnnp_eval_batch_device(
             pot._c, nstruct, off.ctypes.data_as(C.POINTER(C.c_int64)), None, C.c_void_p(Zd.data_ptr()),
             C.c_void_p(posd.data_ptr()), per.ctypes.data_as(C.POINTER(C.c_int32)),
             latf.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(Ed.data_ptr()), C.c_void_p(Fd.data_ptr()),
             C.c_void_p(Ld.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    # the batch as a resident plan: one CUDA-graph launch per step, no host work
+    from hdnnp_b200 import plan as PLm
+
+    bplan = PLm.Plan(pot, structs, precision=prec, margin=0.02, profile=True)
+
+    def step_device():
+        bplan.launch(stream.cuda_stream)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
 
@@ -296,33 +370,34 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed_device_steps(nsteps):
+    def timed_device_steps(nsteps, fn=None, plan=None):
         times = []
         for _ in range(nsteps):
             with torch.cuda.stream(stream):
                 flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            step_device()
+            (fn or step_device)()
             e1.record(stream)
             times.append((e0, e1))
+            if plan is not None:
+                plan.sync(stream.cuda_stream)  # collects the stage events of this launch (outside e0..e1)
         return times
 
     # ---------------- value: inputs resident in HBM
     for _ in range(args.warmup):
         step_device()
-    pot.profile(reset=True)
-    pot.set_profiling(True)
+    bplan.sync(stream.cuda_stream)
+    bplan.profile(reset=True)
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
-    times = timed_device_steps(args.steps)
+    times = timed_device_steps(args.steps, plan=bplan)
     barrier()
     clk = clocks.stop()
-    pot.set_profiling(False)
-    stage_ms, counters = pot.profile(reset=True)
+    stage_ms, counters = bplan.profile(reset=True)
     dev_s = sum(a.elapsed_time(b) for a, b in times) / 1e3
-    launches_per_step = pot.launches()
+    launches_per_step = bplan.info()["kernels_per_launch"]
     t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -333,6 +408,7 @@ def main():
             print(json.dumps({"metric": METRIC, "value": value, "ms_per_step": dev_s / args.steps * 1e3,
                               "precision": args.precision, "stage_ms": stage_ms, "counters": counters,
                               "lean": True}), flush=True)
+        bplan.close()
         pot.close()
         if world > 1:
             dist.destroy_process_group()
@@ -372,14 +448,21 @@ def main():
     # ---------------- comparisons on the same workload (rank 0)
     compare = {}
     if rank == 0:
+        nk = max(2, args.steps // 3)
+        # the same precision without the graph (host set-up + one host read per step)
+        step_eager()
+        torch.cuda.synchronize()
+        et = timed_device_steps(nk, fn=step_eager)
+        torch.cuda.synchronize()
+        compare["batched_eager_" + args.precision] = natoms * len(et) / (sum(a.elapsed_time(b) for a, b in et) / 1e3)
+        # the other precision, as a plan
         other = engine.HDNNP_PREC_FP64 if prec == engine.HDNNP_PREC_MIXED else engine.HDNNP_PREC_MIXED
-        pot.set_precision(other)
-        step_device()
-        torch.cuda.synchronize()
-        ot = timed_device_steps(max(2, args.steps // 3))
-        torch.cuda.synchronize()
+        oplan = PLm.Plan(pot, structs, precision=other, margin=0.02)
+        ot = timed_device_steps(nk, fn=lambda: oplan.launch(stream.cuda_stream))
+        oplan.sync(stream.cuda_stream)
         osec = sum(a.elapsed_time(b) for a, b in ot) / 1e3
         compare["batched_" + ("fp64" if other == engine.HDNNP_PREC_FP64 else "mixed")] = natoms * len(ot) / osec
+        oplan.close()
         pot.set_precision(engine.HDNNP_PREC_FP64)
         rng = np.random.default_rng(7)
         idx = rng.choice(nstruct, size=min(args.plain_sample, nstruct), replace=False)
@@ -398,6 +481,8 @@ def main():
             compare["served"] = serve_leg(pkg, engine, pot, prec, args.serve_seconds)
             compare["served_over_plain_fp64"] = (compare["served"]["saturation"]["atom_steps_per_s"]
                                                  / compare["plain_fp64_per_structure"])
+        if world == 1 and args.md:
+            compare.update(md_legs(pkg, engine, PLm, pot, torch))
 
     # ---------------- roofline of the dominant kernel
     evals = max(counters["evaluations"], 1)
@@ -435,6 +520,7 @@ def main():
                 "gpu_launches": launches_per_step * args.steps,
                 "roofline": roof, "clocks": clk, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
+    bplan.close()
     pot.close()
     if world > 1:
         dist.destroy_process_group()

@@ -588,8 +588,9 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.wshift = pp ? pp->wshift : nullptr;
     b.pos_ref = pp ? pp->pos_ref : nullptr;
     int L = 0;
-    if (c->profile && !pp) {
-        if ((r = collect_profile(c))) return r;
+    if (c->profile) {
+        // a plan collects the stage times of its replays itself (ctx_profile_replay)
+        if (!pp && (r = collect_profile(c))) return r;
         for (auto& e : c->ev)
             if (!e) CUDA_TRY(cudaEventCreate(&e));
         if (!c->stats.p) {
@@ -597,11 +598,20 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             CUDA_TRY(cudaMemset(c->stats.p, 0, 8 * sizeof(unsigned long long)));
         }
         b.stats = c->stats.p;
-        c->host_counts[0] += 1;
-        c->host_counts[1] += natoms;
+        if (!pp) {
+            c->host_counts[0] += 1;
+            c->host_counts[1] += natoms;
+        }
     }
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (pp) CUDA_TRY(cudaStreamIsCapturing(st, &capturing));
     auto mark = [&](int k) -> int {
-        if (c->profile && !pp) CUDA_TRY(cudaEventRecord(c->ev[k], st));
+        if (!c->profile) return HDNNP_OK;
+        // inside a stream capture only an external record becomes a graph node
+        if (capturing == cudaStreamCaptureStatusActive)
+            CUDA_TRY(cudaEventRecordWithFlags(c->ev[k], st, cudaEventRecordExternal));
+        else
+            CUDA_TRY(cudaEventRecord(c->ev[k], st));
         return HDNNP_OK;
     };
     CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
@@ -686,7 +696,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     L += mixed ? launch_forces_and_reduce_fp32(b, D, dEdLat_d != nullptr, st)
                : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
     if ((r = mark(7))) return r;
-    if (c->profile) c->prof_pending = true;
+    if (c->profile && !pp) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     c->launches = L;
@@ -1179,6 +1189,17 @@ int ctx_run_planned(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Z_dev,
                     double* energy_dev, double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan& pp) {
     CUDA_TRY(cudaSetDevice(c->model->device));
     return run_pipeline(c, nstruct, natoms, Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st, &pp);
+}
+
+// A plan replay with profiling has finished: accumulate the stage times of
+// its (last) evaluation and count `evals` evaluations of `atoms` atoms.
+int ctx_profile_replay(hdnnp_ctx* c, long long evals, long long atoms) {
+    if (!c->profile || !c->ev[7]) return HDNNP_OK;
+    c->prof_pending = true;
+    int r = collect_profile(c);
+    c->host_counts[0] += evals;
+    c->host_counts[1] += atoms;
+    return r;
 }
 
 // Device error flags of c's evaluations ([4] ints, flags in [0]).

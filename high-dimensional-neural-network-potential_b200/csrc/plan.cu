@@ -34,6 +34,7 @@ int ctx_plan_setup(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t*
 int ctx_run_planned(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Z_dev, const double* pos_dev,
                     double* energy_dev, double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan& pp);
 int* ctx_status_dev(hdnnp_ctx* c);
+int ctx_profile_replay(hdnnp_ctx* c, long long evals, long long atoms);
 }  // namespace hdnnp
 
 using namespace hdnnp;
@@ -88,7 +89,7 @@ struct hdnnp_plan {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    long long launches = 0;
+    long long launches = 0, launches_synced = 0;
     int kernels_per_launch = 0;
 };
 
@@ -179,6 +180,7 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
     if (cudaSetDevice(p->device) != cudaSuccess) return bail(HDNNP_E_CUDA, "cudaSetDevice failed");
     int r = hdnnp_ctx_create(m, &p->ctx);
     if (!r) r = hdnnp_ctx_set_precision(p->ctx, o->precision);
+    if (!r && o->profile) r = hdnnp_ctx_set_profiling(p->ctx, 1);
     if (r) return bail(r, hdnnp_last_error());
     int nel = 0, zs[128], ns[128];
     double max_rc = 0;
@@ -218,6 +220,7 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
                     "probe evaluation flagged the input (device flags " + std::to_string(f) + ")");
     }
     cudaMemset(p->acc, 0, 2 * sizeof(int));
+    if (o->profile) hdnnp_profile_read(p->ctx, nullptr, nullptr, 1);  // the probe is not a launch
     // capture one launch
     p->pp.upload = false;
     if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
@@ -251,6 +254,12 @@ int hdnnp_plan_sync(hdnnp_plan* p, void* stream, int64_t* list_builds) {
     const cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_error(HDNNP_E_CUDA, cudaGetErrorString(e));
     if (list_builds) *list_builds = p->h_acc[1];
+    if (p->o.profile && p->launches > p->launches_synced) {
+        const long long evals = (p->launches - p->launches_synced) * (p->o.momenta_dev ? p->o.steps_per_launch : 1);
+        const int r = ctx_profile_replay(p->ctx, evals, evals * p->natoms);
+        if (r) return r;
+    }
+    p->launches_synced = p->launches;
     const int f = p->h_acc[0];
     if (f & 1) return set_error(HDNNP_E_INPUT, "atom with an element that is not in the potential");
     if (f & 8) return set_error(HDNNP_E_INPUT, "non-finite position");
@@ -259,6 +268,11 @@ int hdnnp_plan_sync(hdnnp_plan* p, void* stream, int64_t* list_builds) {
     if (f & 2) return set_error(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
     if (f & 16) return set_error(HDNNP_E_TIMEOUT, "tensor-core network kernel: bounded wait expired");
     return HDNNP_OK;
+}
+
+int hdnnp_plan_profile(hdnnp_plan* p, double* stage_ms, int64_t* counters, int reset) {
+    if (!p) return set_error(HDNNP_E_INPUT, "null plan");
+    return hdnnp_profile_read(p->ctx, stage_ms, counters, reset);
 }
 
 int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_per_launch) {

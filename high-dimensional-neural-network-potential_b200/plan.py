@@ -26,7 +26,7 @@ from .engine import HDNNP_PREC_FP64, _check, lib
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("margin", C.c_double), ("skin", C.c_double), ("momenta_dev", C.c_void_p),
                 ("masses_dev", C.c_void_p), ("dt", C.c_double), ("steps_per_launch", C.c_int),
-                ("energy_hist_dev", C.c_void_p)]
+                ("energy_hist_dev", C.c_void_p), ("profile", C.c_int)]
 
 
 def _register():
@@ -38,6 +38,7 @@ def _register():
     L.hdnnp_plan_launch.argtypes = [P, P]
     L.hdnnp_plan_sync.argtypes = [P, P, C.POINTER(C.c_int64)]
     L.hdnnp_plan_info.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.hdnnp_plan_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
     L.hdnnp_plan_free.argtypes = [P]
     L.hdnnp_plan_free.restype = None
     L._plan_registered = True
@@ -46,7 +47,8 @@ def _register():
 
 class Plan:
     def __init__(self, pot, structs, precision: int = HDNNP_PREC_FP64, margin: float = 0.25, skin: float = 0.0,
-                 masses=None, momenta=None, dt: float = 0.0, steps_per_launch: int = 1, want_dEdLat: bool = True):
+                 masses=None, momenta=None, dt: float = 0.0, steps_per_launch: int = 1, want_dEdLat: bool = True,
+                 profile: bool = False):
         import torch
 
         L = _register()
@@ -72,7 +74,7 @@ class Plan:
             self.hist = torch.zeros(steps_per_launch, self.nstruct, dtype=torch.float64, device=dev)
         ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
         self._opts = _Opts(int(precision), float(margin), float(skin), ptr(self.mom), ptr(self.mass), float(dt),
-                           int(steps_per_launch), ptr(self.hist))
+                           int(steps_per_launch), ptr(self.hist), 1 if profile else 0)
         self._per, self._lat = per, lat
         h = C.c_void_p()
         _check(L.hdnnp_plan_create(pot._m, C.byref(self._opts), self.nstruct, off.ctypes.data_as(C.c_void_p),
@@ -94,6 +96,16 @@ class Plan:
         k = C.c_int()
         _check(lib().hdnnp_plan_info(self._h, C.byref(e), C.byref(k)))
         return {"entry_capacity": e.value, "kernels_per_launch": k.value}
+
+    def profile(self, reset: bool = False):
+        """(stage times in ms, work counters) as engine.Hdnnp.profile."""
+        from .engine import Hdnnp
+
+        ms = np.zeros(8)
+        cnt = np.zeros(8, np.int64)
+        _check(lib().hdnnp_plan_profile(self._h, ms.ctypes.data_as(C.POINTER(C.c_double)),
+                                        cnt.ctypes.data_as(C.POINTER(C.c_int64)), 1 if reset else 0))
+        return dict(zip(Hdnnp.STAGES, ms[:7].tolist())), dict(zip(Hdnnp.COUNTERS, cnt[:7].tolist()))
 
     def results(self):
         """(energies (nstruct,), forces (natoms, 3), dEdLat (nstruct, 3, 3) or None) as numpy."""

@@ -197,6 +197,7 @@ typedef struct {
     double dt;               /* MD time step                                           */
     int steps_per_launch;    /* MD steps per launch                                    */
     double* energy_hist_dev; /* NULL or steps_per_launch*nstruct energies per launch    */
+    int profile;             /* 1: stage events captured in the graph (hdnnp_plan_profile) */
 } hdnnp_plan_opts;
 
 int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* opts, int nstruct, const int64_t* atom_off,
@@ -208,6 +209,11 @@ int hdnnp_plan_launch(hdnnp_plan* p, void* stream);
  * last sync; list_builds (may be NULL) = neighbour-list builds among them.  */
 int hdnnp_plan_sync(hdnnp_plan* p, void* stream, int64_t* list_builds);
 int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_per_launch);
+/* Profile of a plan created with profile = 1, as hdnnp_profile_read: stage
+ * times accumulate over the launches that hdnnp_plan_sync collected (the
+ * last evaluation of the last launch before each sync); the work counters
+ * cover every evaluation.                                                     */
+int hdnnp_plan_profile(hdnnp_plan* p, double* stage_ms, int64_t* counters, int reset);
 void hdnnp_plan_free(hdnnp_plan* p);
 
 /* ---------------------------------------------------------------- serving
