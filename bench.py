@@ -249,28 +249,33 @@ def serve_leg(pkg, engine, pot, prec, seconds):
 
 
 def md_legs(pkg, engine, PLm, pot, torch):
-    """Device-resident MD, one CUDA graph per launch (resident plans).
+    """The single-structure workloads, each with the CPU stand-in (the oracle
+    on all host threads) timed beside it.
 
     methylammonium: the reference's example (8 atoms, non-periodic, example
       potential, FP64), velocity Verlet at dt = 20 a.u. from seeded 140 K
-      momenta: 1000 steps as 10 launches of a 100-step graph; per-step
+      momenta: 1000 steps as 10 launches of a 100-step CUDA graph; per-step
       latency.  Beside it the same MD through the plain per-call API (host
       integrator, hdnnp_energy_and_forces every step), as the reference runs it.
+    cell_768: the 768-atom cell, one evaluation per call (FP64 and mixed) and
+      as a resident plan.
     strained_49152: 16x16x16 supercell of the ABX3 cell with a 3 % random
       triclinic strain (seed 2), Maxwell-Boltzmann 300 K (seed 3), 200 steps
-      as 10 launches of 20, 1 Bohr Verlet skin, mixed precision, dt DT_SYNTH.
+      as 10 launches of 20, 1 Bohr Verlet skin, mixed precision, dt DT_SYNTH;
+      the CPU stand-in runs the 8x8x8 cut of the same cell.
     """
     W = pkg.workloads
     out = {}
 
+    st = torch.cuda.Stream()  # events and graph launches on one real stream (not the NULL stream)
+
     def timed(plan, launches):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        builds = 0
-        e0.record()
+        e0.record(st)
         for _ in range(launches):
-            plan.launch(torch.cuda.current_stream().cuda_stream)
-        e1.record()
-        builds += plan.sync(torch.cuda.current_stream().cuda_stream)
+            plan.launch(st.cuda_stream)
+        e1.record(st)
+        builds = plan.sync(st.cuda_stream)
         return e0.elapsed_time(e1) / 1e3, builds
 
     s, m, p0 = W.config_c1(EXAMPLE_DIR)
@@ -289,12 +294,57 @@ def md_legs(pkg, engine, PLm, pot, torch):
         E, F, _ = pot1.energy_and_forces(engine.AtStruct(s["Z"], x))
         p = p + 10.0 * (F + Fl)
     hsec = time.perf_counter() - t0
+    # CPU stand-in: the oracle (all host threads) running the same MD loop
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    om = O.Model(EXAMPLE_DIR)
+    x, p, F = s["pos"].copy(), p0.copy(), om.eval(s["Z"], s["pos"], None, stress=False)["forces"]
+    t0 = time.perf_counter()
+    for _ in range(1000):
+        x = x + p / m[:, None] * 20.0 + 0.5 * F / m[:, None] * 400.0
+        Fl = F
+        F = om.eval(s["Z"], x, None, stress=False)["forces"]
+        p = p + 10.0 * (F + Fl)
+    csec = time.perf_counter() - t0
     out["methylammonium_md"] = {
         "workload": "reference example MD: 8 atoms, FP64, dt 20 a.u., 1000 steps (10 graph launches of 100)",
-        "steps_per_s": 1000 / sec, "us_per_step": sec / 1000 * 1e6, "kernels_per_step": pl.info()["kernels_per_launch"] / 100,
-        "plain_api_steps_per_s": nh / hsec, "plain_api_us_per_step": hsec / nh * 1e6}
+        "steps_per_s": 1000 / sec, "us_per_step": sec / 1000 * 1e6,
+        "kernels_per_step": pl.info()["kernels_per_launch"] / 100,
+        "plain_api_steps_per_s": nh / hsec, "plain_api_us_per_step": hsec / nh * 1e6,
+        "cpu_oracle_steps_per_s": 1000 / csec, "cpu_cores": O.max_threads()}
     pl.close()
     pot1.close()
+
+    # 768-atom cell: one structure per call (FP64 and mixed) and as a plan (graph)
+    s2 = W.config_c2()
+    ats2 = engine.AtStruct(s2["Z"], s2["pos"], s2["lat"])
+    c2 = {"workload": "768-atom ABX3 4x4x4 cell (seed 1), E+F+stress"}
+    for name, prec in (("fp64", engine.HDNNP_PREC_FP64), ("mixed", engine.HDNNP_PREC_MIXED)):
+        pot.set_precision(prec)
+        pot.energy_and_forces(ats2, dEdLat=True)
+        ts = []
+        for _ in range(20):
+            t0 = time.perf_counter()
+            pot.energy_and_forces(ats2, dEdLat=True)
+            ts.append(time.perf_counter() - t0)
+        c2[f"plain_api_{name}_ms"] = float(np.median(ts) * 1e3)
+        p2 = PLm.Plan(pot, [s2], precision=prec)
+        timed(p2, 2)
+        sec, _ = timed(p2, 20)
+        c2[f"plan_{name}_ms"] = sec / 20 * 1e3
+        p2.close()
+    pot.set_precision(engine.HDNNP_PREC_FP64)
+    om2 = O.Model(POT_DIR)
+    om2.eval(s2["Z"], s2["pos"], s2["lat"])
+    ts = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        om2.eval(s2["Z"], s2["pos"], s2["lat"])
+        ts.append(time.perf_counter() - t0)
+    c2["cpu_oracle_ms"] = float(np.median(ts) * 1e3)
+    c2["atom_steps_per_s"] = {k[:-3]: 768 / (v / 1e3) for k, v in c2.items() if k.endswith("_ms")}
+    out["cell_768"] = c2
 
     s3 = W.config_c3()
     m3, p3 = W.maxwell_boltzmann(s3["Z"], 300.0, 3)
@@ -303,10 +353,19 @@ def md_legs(pkg, engine, PLm, pot, torch):
     timed(pl3, 1)
     sec, builds = timed(pl3, 10)
     nat = len(s3["Z"])
+    # CPU stand-in on the 8x8x8 cut of the same strained cell (per-atom rate)
+    s3c = W.config_c3(n=8)
+    om2.eval(s3c["Z"], s3c["pos"], s3c["lat"])
+    t0 = time.perf_counter()
+    for _ in range(2):
+        om2.eval(s3c["Z"], s3c["pos"], s3c["lat"])
+    c3sec = (time.perf_counter() - t0) / 2
     out["strained_49152_md"] = {
         "workload": f"{nat} atoms, 3% triclinic strain, 300 K, 200 MD steps (10 graph launches of 20), "
                     f"1 Bohr Verlet skin, mixed precision, dt {DT_SYNTH} a.u.",
-        "atom_steps_per_s": nat * 200 / sec, "ms_per_step": sec / 200 * 1e3, "list_builds": builds}
+        "atom_steps_per_s": nat * 200 / sec, "ms_per_step": sec / 200 * 1e3, "list_builds": builds,
+        "cpu_oracle_atom_steps_per_s": len(s3c["Z"]) / c3sec,
+        "cpu_sample": f"8x8x8 cut ({len(s3c['Z'])} atoms), E+F+stress, FP64"}
     pl3.close()
     return out
 
