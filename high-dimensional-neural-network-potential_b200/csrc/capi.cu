@@ -184,6 +184,7 @@ struct hdnnp_ctx {
         el_count, el_start, el_atoms, scan_tmp, status;
     DevBuf<double> pos, wpos, G, dEdG, atE, gent, gself, vir, force, energy, dEdLat;
     DevBuf<float> Gf, dEdGf, atEf, gentf, gselff, virf;  // mixed-precision intermediates
+    DevBuf<double> cm_acc, cm_E, cm_std;                  // committee: dE/dG sum, member energies, std
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -200,7 +201,9 @@ struct hdnnp_ctx {
         for (auto* b : {&Z, &sid, &elem, &cell_of, &cell_cnt, &cell_start, &cell_atoms, &nei_cnt, &nei_off, &nei_j,
                         &nei_s, &nei_rev, &el_count, &el_start, &el_atoms, &scan_tmp, &status})
             b->release();
-        for (auto* b : {&pos, &wpos, &G, &dEdG, &atE, &gent, &gself, &vir, &force, &energy, &dEdLat}) b->release();
+        for (auto* b : {&pos, &wpos, &G, &dEdG, &atE, &gent, &gself, &vir, &force, &energy, &dEdLat, &cm_acc, &cm_E,
+                        &cm_std})
+            b->release();
         for (auto* b : {&Gf, &dEdGf, &atEf, &gentf, &gselff, &virf}) b->release();
         info.release();
         stats.release();
@@ -524,7 +527,8 @@ int collect_profile(hdnnp_ctx* c) {
 // Core pipeline; inputs already on the device in c->Z / c->pos (or external
 // device pointers), structure set-up in c->hinfo.
 int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const double* posd, double* energy_d,
-                 double* force_d, double* dEdLat_d, cudaStream_t st, PipePlan* pp = nullptr) {
+                 double* force_d, double* dEdLat_d, cudaStream_t st, PipePlan* pp = nullptr,
+                 const Committee* cm = nullptr) {
     hdnnp_model* m = c->model;
     DevModel D = m->dev;
     // runtime-zeta variant of a compiled-zeta shape (same product layout)
@@ -678,6 +682,12 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");
         if (mlp_smem_bytes(D, mixed ? sizeof(float) : sizeof(double)) > 220 * 1024)
             return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+        if (cm) {
+            for (int q = 0; q < cm->k; ++q)
+                if (mlp_smem_bytes(*cm->members[q], mixed ? sizeof(float) : sizeof(double)) > 220 * 1024)
+                    return fail(HDNNP_E_CAPACITY, "committee member " + std::to_string(q) + ": network too wide");
+            if ((r = c->cm_acc.ensure(N * D.nsf_max)) || (r = c->cm_E.ensure((size_t)cm->k * nstruct))) return r;
+        }
     }
     if ((r = mark(1))) return r;  // after the host read: stage 1 starts here
     L += launch_neighbour_build_b(b, D, st);
@@ -686,7 +696,9 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if ((r = mark(3))) return r;
     L += fast ? launch_sf_values_fast(b, D, mixed, st) : launch_sf_values(b, D, st);
     if ((r = mark(4))) return r;
-    if (mixed && D.tc_ok && !c->mlp_simt)
+    if (cm)
+        L += launch_committee_networks(b, *cm, mixed, !c->mlp_simt, c->cm_acc.p, c->cm_E.p, st);
+    else if (mixed && D.tc_ok && !c->mlp_simt)
         L += launch_mlp_tc(b, D, st);
     else
         L += mixed ? launch_mlp_fp32(b, D, st) : launch_mlp(b, D, st);
@@ -695,6 +707,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if ((r = mark(6))) return r;
     L += mixed ? launch_forces_and_reduce_fp32(b, D, dEdLat_d != nullptr, st)
                : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
+    if (cm) L += launch_committee_finish(b, *cm, c->cm_E.p, st);  // mean energies (and std)
     if ((r = mark(7))) return r;
     if (c->profile && !pp) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
@@ -873,6 +886,65 @@ int hdnnp_energy_and_forces(hdnnp_ctx* c, int nat, const int32_t* Z, const doubl
     int32_t per = periodic ? 1 : 0;
     double dummy[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     return hdnnp_eval_batch(c, 1, off, Z, pos, &per, lat ? lat : dummy, energy, force, dEdLat);
+}
+
+int hdnnp_committee_eval_batch(hdnnp_ctx* c, hdnnp_model* const* members, int nmembers, int nstruct,
+                               const int64_t* atom_off, const int32_t* Z, const double* pos, const int32_t* periodic,
+                               const double* lat, double* energy, double* force, double* dEdLat, double* std_dev) {
+    if (!c || !members || nmembers < 1 || nstruct <= 0 || !atom_off || !Z || !pos || !lat || !energy || !force)
+        return fail(HDNNP_E_INPUT, "null argument, empty batch or empty committee");
+    if (members[0] != c->model)
+        return fail(HDNNP_E_INPUT, "the context must belong to the first member (it provides the symmetry functions)");
+    const HostModel& H0 = c->model->host;
+    std::vector<const DevModel*> dms((size_t)nmembers);
+    for (int q = 0; q < nmembers; ++q) {
+        const hdnnp_model* mq = members[q];
+        if (!mq) return fail(HDNNP_E_INPUT, "committee member " + std::to_string(q) + " is null");
+        if (mq->device != c->model->device)
+            return fail(HDNNP_E_INPUT, "committee member " + std::to_string(q) + " lives on another device");
+        const HostModel& Hq = mq->host;
+        if (Hq.el.size() != H0.el.size())
+            return fail(HDNNP_E_INPUT, "committee member " + std::to_string(q) + " has other elements");
+        for (size_t e = 0; e < H0.el.size(); ++e)
+            if (Hq.el[e].z != H0.el[e].z || Hq.el[e].net.empty() || Hq.el[e].net[0].nin != (int)H0.el[e].sfs.size())
+                return fail(HDNNP_E_INPUT, "committee member " + std::to_string(q) +
+                                               ": elements or network input widths differ from the first member's "
+                                               "symmetry functions");
+        dms[q] = &mq->dev;
+    }
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    int r = prepare_structs(c, nstruct, atom_off, Z, pos, periodic, lat, true);
+    if (r) return r;
+    const int natoms = (int)atom_off[nstruct];
+    const size_t N = natoms;
+    cudaStream_t st = c->stream;
+    if ((r = c->Z.ensure(N)) || (r = c->pos.ensure(3 * N)) || (r = c->force.ensure(3 * N)) ||
+        (r = c->energy.ensure(nstruct)) || (r = c->dEdLat.ensure(9 * (size_t)nstruct)) ||
+        (r = c->cm_std.ensure(nstruct)))
+        return r;
+    CUDA_TRY(cudaMemcpyAsync(c->Z.p, Z, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    Committee cm{dms.data(), nmembers, c->cm_std.p};
+    r = run_pipeline(c, nstruct, natoms, c->Z.p, c->pos.p, c->energy.p, c->force.p, dEdLat ? c->dEdLat.p : nullptr,
+                     st, nullptr, &cm);
+    if (r) return r;
+    CUDA_TRY(cudaMemcpyAsync(energy, c->energy.p, sizeof(double) * nstruct, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(force, c->force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
+    if (dEdLat) CUDA_TRY(cudaMemcpyAsync(dEdLat, c->dEdLat.p, sizeof(double) * 9 * nstruct, cudaMemcpyDeviceToHost, st));
+    if (std_dev) CUDA_TRY(cudaMemcpyAsync(std_dev, c->cm_std.p, sizeof(double) * nstruct, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return check_status(c);
+}
+
+int hdnnp_committee_energy_and_forces(hdnnp_ctx* c, hdnnp_model* const* members, int nmembers, int nat,
+                                      const int32_t* Z, const double* pos, int periodic, const double* lat,
+                                      double* energy, double* force, double* dEdLat, double* std_dev) {
+    if (dEdLat && !periodic) return fail(HDNNP_E_INPUT, "dEdLat needs a periodic structure");
+    int64_t off[2] = {0, nat};
+    int32_t per = periodic ? 1 : 0;
+    double dummy[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    return hdnnp_committee_eval_batch(c, members, nmembers, 1, off, Z, pos, &per, lat ? lat : dummy, energy, force,
+                                      dEdLat, std_dev);
 }
 
 int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stress) {

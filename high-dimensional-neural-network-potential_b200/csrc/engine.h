@@ -183,6 +183,17 @@ struct PipePlan {
     double* pos_ref = nullptr;
 };
 
+// Committee of potentials (committee.cu; globalHdnnpEnergyAndForces,
+// globalHdnnps.f90:31-70): neighbour lists and symmetry functions of the
+// first member, every member's networks on them; dE/dG is averaged before the
+// (linear) force/virial contraction, energies are averaged per structure and
+// their population standard deviation is written to std_dev[nstruct].
+struct Committee {
+    const DevModel* const* members;  // host array of K device models; members[0] gives the SFs
+    int k;
+    double* std_dev;                 // device [nstruct] or null
+};
+
 // packed image shift: three signed 8-bit lattice multiples
 __host__ __device__ inline int pack_shift(int x, int y, int z) {
     return (x & 0xff) | ((y & 0xff) << 8) | ((z & 0xff) << 16);
@@ -212,6 +223,14 @@ int launch_mlp_fp32(const Batch& b, const DevModel& m, cudaStream_t s);
 int launch_forces_and_reduce_fp32(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s);
 size_t mlp_smem_bytes(const DevModel& m, size_t elem);
 int launch_mlp_tc(const Batch& b, const DevModel& m, cudaStream_t s);
+// per-structure compensated sums of the atomic energies (FP64 or FP32 atE) into out[nstruct]
+int launch_struct_energies(const Batch& b, bool fp32, double* out, cudaStream_t s);
+// Committee: every member's network (acc: natoms*nsf_max accumulator of the
+// working precision, Ek: K*nstruct member energies), then dE/dG = mean; the
+// finish step writes the mean energies and their standard deviation.
+int launch_committee_networks(const Batch& b, const Committee& cm, bool mixed, bool use_tc, void* acc, double* Ek,
+                              cudaStream_t s);
+int launch_committee_finish(const Batch& b, const Committee& cm, const double* Ek, cudaStream_t s);
 size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);

@@ -104,7 +104,38 @@ __global__ void __launch_bounds__(kRedThreads) k_struct_reduce(Batch b, int want
     }
 }
 
+// Compensated per-structure sum of the atomic energies only (committee members).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_struct_energy(Batch b, const T* atE, double* out) {
+    __shared__ double se[kRedThreads], sc[kRedThreads];
+    const StructInfo& S = b.info[blockIdx.x];
+    KSum k{0.0, 0.0};
+    for (int i = threadIdx.x; i < S.nat; i += kRedThreads) k.add((double)atE[S.atom_off + i]);
+    se[threadIdx.x] = k.s;
+    sc[threadIdx.x] = k.c;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            KSum a{se[threadIdx.x], sc[threadIdx.x]};
+            KSum o{se[threadIdx.x + w], sc[threadIdx.x + w]};
+            a.merge(o);
+            se[threadIdx.x] = a.s;
+            sc[threadIdx.x] = a.c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = se[0] + sc[0];
+}
+
 }  // namespace
+
+int launch_struct_energies(const Batch& b, bool fp32, double* out, cudaStream_t s) {
+    if (fp32)
+        k_struct_energy<float><<<b.nstruct, kRedThreads, 0, s>>>(b, b.atEf, out);
+    else
+        k_struct_energy<double><<<b.nstruct, kRedThreads, 0, s>>>(b, b.atE, out);
+    return 1;
+}
 
 int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s) {
     (void)m;

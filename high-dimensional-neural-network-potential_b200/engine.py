@@ -11,6 +11,9 @@ hdnnpEnergyAndForces(h, ats,   ``h.energy_and_forces(ats, dEdLat=True)``
   energy, force, dEdLat)        -> (energy, force(nat,3), dEdLat(3,3)) (:333)
 type atStruct                  ``AtStruct``         (atomicStructure.f90:17)
 dEdLat2Stress(lat, dEdLat, s)  ``dEdLat_to_stress`` (atomicStructure.f90:679)
+globalHdnnpEnergyAndForces(    ``h.committee_energy_and_forces(members, ats)``
+  ats, energy, forces,          -> (energy, forces, dEdLat, std)
+  dEdLat, std)                  (globalHdnnps.f90:31)
 =============================  ==============================================
 
 Errors that make the reference ``stop`` raise ``HdnnpError`` here.  Arrays
@@ -73,6 +76,8 @@ def lib():
     L.hdnnp_last_launch_count.argtypes = [P, C.POINTER(C.c_int)]
     L.hdnnp_ctx_set_profiling.argtypes = [P, C.c_int]
     L.hdnnp_profile_read.argtypes = [P, D, I64, C.c_int]
+    L.hdnnp_committee_energy_and_forces.argtypes = [P, P, C.c_int, C.c_int, I, D, C.c_int, D, D, D, D, D]
+    L.hdnnp_committee_eval_batch.argtypes = [P, P, C.c_int, C.c_int, I64, I, D, I, D, D, D, D, D]
     L.hdnnp_server_create.argtypes = [P, P, C.POINTER(C.c_void_p)]
     L.hdnnp_server_destroy.argtypes = [P]
     L.hdnnp_server_destroy.restype = None
@@ -197,6 +202,39 @@ class Hdnnp:
         lat = np.concatenate([_lat_flat(s["lat"]) for s in structs])
         per = np.array([0 if s["lat"] is None else 1 for s in structs], np.int32)
         return self.eval_batch_arrays(off, Z, pos, per, lat, dEdLat)
+
+    # ------------------------------------------------------------------ committee
+    def committee_energy_and_forces(self, members: Sequence["Hdnnp"], ats: AtStruct, dEdLat: bool = False):
+        """globalHdnnpEnergyAndForces (globalHdnnps.f90:31): members[0] must be
+        this potential (it provides the symmetry functions).  Returns mean
+        energy, mean forces (nat, 3), mean dE/dh (3, 3) or None, and the
+        standard deviation of the member energies."""
+        n = ats.nat
+        E, sd = C.c_double(), C.c_double()
+        F = np.zeros((n, 3))
+        dl = np.zeros(9) if dEdLat else None
+        arr = (C.c_void_p * len(members))(*[m._m for m in members])
+        _check(lib().hdnnp_committee_energy_and_forces(
+            self._c, arr, len(members), n, _ip(ats.el), _dp(ats.ats), 1 if ats.periodic else 0,
+            _dp(_lat_flat(ats.lat)), C.byref(E), _dp(F), _dp(dl), C.byref(sd)))
+        return E.value, F, (dl.reshape(3, 3, order="F") if dl is not None else None), sd.value
+
+    def committee_eval_batch(self, members: Sequence["Hdnnp"], structs: Sequence[dict], dEdLat: bool = True):
+        """Committee over a batch: dict of energy, forces, dEdLat, std."""
+        off = np.zeros(len(structs) + 1, np.int64)
+        off[1:] = np.cumsum([len(s["Z"]) for s in structs])
+        Z = np.ascontiguousarray(np.concatenate([s["Z"] for s in structs]), dtype=np.int32)
+        pos = np.ascontiguousarray(np.concatenate([s["pos"] for s in structs]), dtype=np.float64)
+        lat = np.concatenate([_lat_flat(s["lat"]) for s in structs])
+        per = np.array([0 if s["lat"] is None else 1 for s in structs], np.int32)
+        ns = len(structs)
+        out = {"energy": np.zeros(ns), "forces": np.zeros((int(off[-1]), 3)),
+               "dEdLat": np.zeros(9 * ns) if dEdLat else None, "std": np.zeros(ns)}
+        arr = (C.c_void_p * len(members))(*[m._m for m in members])
+        _check(lib().hdnnp_committee_eval_batch(
+            self._c, arr, len(members), ns, off.ctypes.data_as(C.POINTER(C.c_int64)), _ip(Z), _dp(pos), _ip(per),
+            _dp(lat), _dp(out["energy"]), _dp(out["forces"]), _dp(out["dEdLat"]), _dp(out["std"])))
+        return out
 
     def eval_batch_arrays(self, off, Z, pos, per, lat_flat, dEdLat=True, out=None):
         ns = len(off) - 1

@@ -113,6 +113,25 @@ int hdnnp_eval_batch_device(hdnnp_ctx* c, int nstruct, const int64_t* atom_off_h
                             const double* lat_host, double* energy_dev, double* force_dev, double* dEdLat_dev,
                             void* stream);
 
+/* ---------------------------------------------------------------- committee
+ * Replaces globalHdnnpEnergyAndForces(ats, energy, forces, dEdLat, std)
+ * (globalHdnnps.f90:31-70): neighbour lists and symmetry functions -- with
+ * their scaling -- come from members[0] (:47, :51), and every member's
+ * networks run on them (:55-57); energy, forces and dEdLat are the member
+ * means and std the population standard deviation of the member energies
+ * (:60-68).  `c` must be a context of members[0]; every member must have the
+ * same elements and a network input as wide as members[0]'s symmetry-function
+ * list (the reference assumes this silently).  The members' dE/dG are averaged
+ * before the one force/virial contraction (linear; equal within rounding to
+ * averaging member forces).  std may be NULL.  The batch form takes the
+ * arrays of hdnnp_eval_batch plus std[nstruct].                              */
+int hdnnp_committee_energy_and_forces(hdnnp_ctx* c, hdnnp_model* const* members, int nmembers, int nat,
+                                      const int32_t* Z, const double* pos, int periodic, const double* lat,
+                                      double* energy, double* force, double* dEdLat, double* std);
+int hdnnp_committee_eval_batch(hdnnp_ctx* c, hdnnp_model* const* members, int nmembers, int nstruct,
+                               const int64_t* atom_off, const int32_t* Z, const double* pos, const int32_t* periodic,
+                               const double* lat, double* energy, double* force, double* dEdLat, double* std);
+
 /* ---------------------------------------------------------------- no-allocation variant
  * No counterpart in the reference.  The same evaluation as
  * hdnnp_energy_and_forces (host arrays in and out, same arguments and
