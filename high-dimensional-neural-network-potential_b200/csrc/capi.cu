@@ -481,6 +481,8 @@ int upload_model(hdnnp_model* m) {
     D.rc = (const double*)(base + o_rc);
     D.nsf = (const int*)(base + o_nsf);
     D.g2_off = (const int*)(base + o_g2o);
+    D.g2max = 0;
+    for (int c = 0; c < nel; ++c) D.g2max = std::max(D.g2max, g2_off[(size_t)c * nel + nel] - g2_off[(size_t)c * nel]);
     D.g2 = (const SF2*)(base + o_g2);
     D.g4_off = (const int*)(base + o_g4o);
     D.g4 = (const SF4*)(base + o_g4);
@@ -676,7 +678,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     {
         int mm = ((b.mmax + 31) / 32) * 32;
         const size_t sf_smem =
-            fast ? sf_fast_smem_per_warp(mm, D.nsf_max, D.nblk, fast_shape_p(D.fast), true, mixed) * 4
+            fast ? sf_fast_smem_per_warp(mm, D.g2max, D.nblk, fast_shape_p(D.fast), true, mixed) * 4
                    : sf_smem_per_warp(mm, true) * 4;
         if (sf_smem > 220 * 1024 || (fast && mm > 1024))
             return fail(HDNNP_E_CAPACITY, "too many neighbours per atom for the symmetry-function kernels");

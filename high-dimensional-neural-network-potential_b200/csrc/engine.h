@@ -62,6 +62,7 @@ struct DevModel {
     const double* rc;         // [nel] cutoff of each centre element
     const int* nsf;           // [nel]
     const int* g2_off;        // [nel*nel+1]
+    int g2max;                // most radial SFs of one centre element
     const SF2* g2;
     const int* g4_off;        // [nel*nblk+1]
     const SF4* g4;
@@ -247,6 +248,6 @@ inline int fast_shape_p(int id) { return kFastShapes[id][0] * kFastShapes[id][1]
 // Fast (product-space) symmetry-function kernels, FP64 (T = double) or FP32.
 int launch_sf_values_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t s);
 int launch_sf_gradients_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t s);
-size_t sf_fast_smem_per_warp(int mmax, int nsf, int nblk, int P, bool grad, bool fp32);
+size_t sf_fast_smem_per_warp(int mmax, int g2max, int nblk, int P, bool grad, bool fp32);
 
 }  // namespace hdnnp

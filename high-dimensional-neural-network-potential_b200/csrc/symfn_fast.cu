@@ -27,6 +27,10 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;
+// Resident blocks per SM the FP32 kernels are compiled for (registers): 7 x 4
+// warps for the value pass, 8 x 4 for the gradient pass (a few bytes of
+// spill), which the shared memory of a launch sized for 64 neighbours also
+// allows.  The FP64 kernels keep their registers (4 blocks).
 
 template <typename T>
 struct alignas(4 * sizeof(T)) V4 {
@@ -38,7 +42,7 @@ __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15);
 template <typename T>
 struct FSmem {
     V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
-    V4<double>* dd; // FP64 dx, dy, dz (FP32 form only; aliases nb in FP64)
+    V4<float>* lo;  // FP32 form: FP64 d - (float)d per component (FP64 d = nb + lo)
     V4<T>* ax;      // fc, dfc/r, 1/r, -
     V4<T>* g;       // gradient accumulators (pass 2)
     int* ent;       // entry index of a slot (pass 2)
@@ -46,24 +50,24 @@ struct FSmem {
     unsigned* queue;
     int* est;
     int* cur;
-    T* w;           // dE/dG / width (pass 2)
+    T* w2;          // dE/dG / width of the centre's radial SFs (pass 2)
     T* WA;          // [nblk][P] (pass 2)
     T* WC;
     T* red;         // [32][P+1] (pass 1)
 };
 
 template <typename T>
-__host__ __device__ inline size_t fast_warp_bytes(int mm, int nsf, int nblk, int P, bool grad) {
+__host__ __device__ inline size_t fast_warp_bytes(int mm, int g2max, int nblk, int P, bool grad) {
     size_t b = a16(sizeof(V4<T>) * mm) * 2;
-    if (sizeof(T) == 4) b += a16(sizeof(V4<double>) * mm);
-    if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * nsf) + 2 * a16(sizeof(T) * nblk * P);
+    if (sizeof(T) == 4) b += a16(sizeof(V4<float>) * mm);
+    if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
     else b += a16(sizeof(T) * 32 * (P + 1));
     b += a16(mm) + 64 * sizeof(unsigned) + a16(sizeof(int) * (kMaxEl + 1)) + a16(sizeof(int) * kMaxEl);
     return b;
 }
 
 template <typename T>
-__device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int nsf, int nblk, int P, bool grad) {
+__device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int g2max, int nblk, int P, bool grad) {
     FSmem<T> s{};
     auto take = [&](size_t bytes) {
         unsigned char* q = p;
@@ -71,12 +75,12 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int nsf, int nblk, i
         return q;
     };
     s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
-    s.dd = sizeof(T) == 4 ? (V4<double>*)take(sizeof(V4<double>) * mm) : (V4<double>*)s.nb;
+    s.lo = sizeof(T) == 4 ? (V4<float>*)take(sizeof(V4<float>) * mm) : nullptr;
     s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
     if (grad) {
         s.g = (V4<T>*)take(sizeof(V4<T>) * mm);
         s.ent = (int*)take(sizeof(int) * mm);
-        s.w = (T*)take(sizeof(T) * nsf);
+        s.w2 = (T*)take(sizeof(T) * g2max);
         s.WA = (T*)take(sizeof(T) * nblk * P);
         s.WC = (T*)take(sizeof(T) * nblk * P);
     } else {
@@ -87,6 +91,29 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int nsf, int nblk, i
     s.est = (int*)take(sizeof(int) * (kMaxEl + 1));
     s.cur = (int*)take(sizeof(int) * kMaxEl);
     return s;
+}
+
+// P consecutive weights of one block from shared memory in 16-byte loads
+// (P is a multiple of 4; each block's tensor starts on a 16-byte boundary).
+template <int P>
+__device__ __forceinline__ void ldvec(const float* p, float (&w)[P]) {
+#pragma unroll
+    for (int q = 0; q < P / 4; ++q) {
+        const float4 v = reinterpret_cast<const float4*>(p)[q];
+        w[4 * q] = v.x;
+        w[4 * q + 1] = v.y;
+        w[4 * q + 2] = v.z;
+        w[4 * q + 3] = v.w;
+    }
+}
+template <int P>
+__device__ __forceinline__ void ldvec(const double* p, double (&w)[P]) {
+#pragma unroll
+    for (int q = 0; q < P / 2; ++q) {
+        const double2 v = reinterpret_cast<const double2*>(p)[q];
+        w[2 * q] = v.x;
+        w[2 * q + 1] = v.y;
+    }
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -221,7 +248,9 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
                 dfc = -3.0 / (rc * r) * (tt - tt * tt);
             }
             s.nb[slot] = V4<T>{(T)dx, (T)dy, (T)dz, (T)r};
-            if (sizeof(T) == 4) s.dd[slot] = V4<double>{dx, dy, dz, r};
+            if (sizeof(T) == 4)
+                s.lo[slot] = V4<float>{(float)(dx - (double)(float)dx), (float)(dy - (double)(float)dy),
+                                       (float)(dz - (double)(float)dz), 0.0f};
             s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)(1.0 / r), (T)0};
             s.el[slot] = (unsigned char)el;
             if (kGrad) {
@@ -264,8 +293,20 @@ __device__ __forceinline__ void fpair(int c, int sa, int na, int sb, int nb, boo
 // SFs can have tiny scaling ranges and therefore large weights).
 template <typename T>
 __device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d, T rc, T rjk) {
-    const V4<double> a = s.dd[j], b = s.dd[k];
-    const double cx = b.x - a.x, cy = b.y - a.y, cz = b.z - a.z;
+    double cx, cy, cz;
+    if (sizeof(T) == 4) {
+        // FP64 relative vectors rebuilt exactly from the FP32 value and residual
+        const V4<T> a = s.nb[j], b = s.nb[k];
+        const V4<float> al = s.lo[j], bl = s.lo[k];
+        cx = ((double)b.x + (double)bl.x) - ((double)a.x + (double)al.x);
+        cy = ((double)b.y + (double)bl.y) - ((double)a.y + (double)al.y);
+        cz = ((double)b.z + (double)bl.z) - ((double)a.z + (double)al.z);
+    } else {
+        const V4<T> a = s.nb[j], b = s.nb[k];
+        cx = (double)b.x - (double)a.x;
+        cy = (double)b.y - (double)a.y;
+        cz = (double)b.z - (double)a.z;
+    }
     const double D = rc2d - (cx * cx + cy * cy + cz * cz);
     return D > 0.0 ? (T)D / (rc * (rc + rjk)) : (T)0;
 }
@@ -364,11 +405,11 @@ __device__ __forceinline__ int n_eta(const DevModel& m) {
 
 // ---------------------------------------------------------------- pass 1
 template <typename T, class S>
-__global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, int mm) {
+__global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fast(Batch b, DevModel m, int mm, int mlo, int last) {
     constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, false), mm, m.nsf_max,
+    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.g2max, m.nblk, P, false), mm, m.g2max,
                            m.nblk, P, false);
     const int nel = m.nel;
     T* Gout = Buf<T>::G(b);
@@ -377,10 +418,12 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
         const int c = b.elem[i];
         if (c < 0) continue;
         const int M = b.nei_off[i + 1] - b.nei_off[i];
+        // this launch takes the atoms with mlo < M <= mm (see run_spec)
         if (M > mm) {
-            if (lane == 0) atomicOr(&b.status[0], 4);
+            if (last && lane == 0) atomicOr(&b.status[0], 4);
             continue;
         }
+        if (M <= mlo) continue;
         const int Ms = fstage<T, false>(b, m, i, c, s, lane, M);
         const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
         const double rc2d = m.rc[c] * m.rc[c];
@@ -510,11 +553,11 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfv_fast(Batch b, DevModel m, i
 
 // ---------------------------------------------------------------- pass 2
 template <typename T, class S>
-__global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, int mm) {
+__global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fast(Batch b, DevModel m, int mm, int mlo, int last) {
     constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, P, true), mm, m.nsf_max,
+    FSmem<T> s = fcarve<T>(smem_raw + wib * fast_warp_bytes<T>(mm, m.g2max, m.nblk, P, true), mm, m.g2max,
                            m.nblk, P, true);
     const int nel = m.nel;
     const T* dEdG = Buf<T>::dEdG(b);
@@ -523,24 +566,31 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
         const int c = b.elem[i];
         if (c < 0) continue;
         const int M = b.nei_off[i + 1] - b.nei_off[i];
+        // this launch takes the atoms with mlo < M <= mm (see run_spec)
         if (M > mm) {
-            if (lane == 0) atomicOr(&b.status[0], 4);
+            if (last && lane == 0) atomicOr(&b.status[0], 4);
             continue;
         }
+        if (M <= mlo) continue;
         const int Ms = fstage<T, true>(b, m, i, c, s, lane, M);
         const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
         const double rc2d = m.rc[c] * m.rc[c];
-        const int nsf = m.nsf[c];
-        for (int q = lane; q < nsf; q += 32)
-            s.w[q] = (T)((double)dEdG[(size_t)i * m.nsf_max + q] / m.swidth[(size_t)c * m.nsf_max + q]);
-        __syncwarp();
+        // w_s = dE/dG_s / width_s: radial SFs staged per slot of g2, angular
+        // ones folded into the product-space weight tensors of each block
+        const T* dEdGi = dEdG + (size_t)i * m.nsf_max;
+        const double* widc = m.swidth + (size_t)c * m.nsf_max;
+        const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
+        for (int f = r0 + lane; f < r1; f += 32) {
+            const int sf = m.g2[f].sf;
+            s.w2[f - r0] = (T)((double)dEdGi[sf] / widc[sf]);
+        }
         for (int q = lane; q < m.nblk * P; q += 32) {
             const int t = q / P, p = q % P;
             const int sf = m.pmap[((size_t)c * m.nblk + t) * P + p];
             T wa = (T)0, wc = (T)0;
             if (sf >= 0) {
                 const int l = p / (NZ * NE), z = (p / NE) % NZ;
-                wa = s.w[sf] * (T)m.pfz[z];
+                wa = (T)((double)dEdGi[sf] / widc[sf]) * (T)m.pfz[z];
                 wc = wa * (T)m.lam[l] * (T)m.zet[z];
             }
             s.WA[q] = wa;
@@ -559,7 +609,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                 const SF2 q = m.g2[f];
                 const T eta = (T)q.eta, xr = d.w - (T)q.rs;
                 const T e = xexp(-eta * xr * xr);
-                coef += s.w[q.sf] * (-e * x.y + (T)2 * eta * xr * x.z * e * x.x);
+                coef += s.w2[f - r0] * (-e * x.y + (T)2 * eta * xr * x.z * e * x.x);
             }
             V4<T> g = s.g[t];
             g.x += coef * d.x;
@@ -598,9 +648,13 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                 const bool flush_all = last_blk && cb + 32 >= ncand;
                 while (qlen >= 32 || (flush_all && qlen > 0)) {
                     const int n = qlen < 32 ? qlen : 32;
+                    // dE/dr_j of this lane's pair, summed over runs of equal j below
+                    int pj = -1 - lane;
+                    T gjx = (T)0, gjy = (T)0, gjz = (T)0;
                     if (lane < n) {
                         const unsigned pk = s.queue[lane];
-                        const int pj = pk & 0x3ff, pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
+                        pj = pk & 0x3ff;
+                        const int pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
                         const V4<T> a = s.nb[pj], bq = s.nb[pq];
                         const V4<T> xa = s.ax[pj], xb = s.ax[pq];
                         const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
@@ -624,8 +678,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                         T SA[NE], SC[NE];
 #pragma unroll
                         for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
-                        const T* wa = s.WA + pt * P;
-                        const T* wc = s.WC + pt * P;
+                        T wa[P], wc[P];
+                        ldvec<P>(s.WA + pt * P, wa);
+                        ldvec<P>(s.WC + pt * P, wc);
 #pragma unroll
                         for (int l = 0; l < NL; ++l) {
                             T Tz[NZ], Tp[NZ];
@@ -648,18 +703,43 @@ __global__ void __launch_bounds__(32 * kWarps) k_sfg_fast(Batch b, DevModel m, i
                         const T B2 = (T)2 * B * fcp, Cf = C * fcp;
                         const T pj1 = A * fk * fj * dfjk, pj2 = A * fk * dfj * fjk;
                         const T pk1 = A * fj * fk * dfjk, pk2 = A * fj * dfk * fjk;
-                        const T gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
-                        const T gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
-                        const T gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
+                        gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
+                        gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
+                        gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
                         const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
                         const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
                         const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
-                        atomicAdd(&s.g[pj].x, gjx);
-                        atomicAdd(&s.g[pj].y, gjy);
-                        atomicAdd(&s.g[pj].z, gjz);
                         atomicAdd(&s.g[pq].x, gkx);
                         atomicAdd(&s.g[pq].y, gky);
                         atomicAdd(&s.g[pq].z, gkz);
+                    }
+                    // Queue order is enumeration order, so pairs sharing j sit in
+                    // contiguous lanes: a segmented suffix sum (fixed shuffle order)
+                    // leaves each run's total in its first lane, which alone
+                    // updates slot j -- instead of one conflicting atomic per lane.
+                    {
+                        // every lane executes the shuffle (no short-circuit around it)
+                        const int prev_j = __shfl_up_sync(kFull, pj, 1);
+                        const bool head = lane == 0 || prev_j != pj;
+                        const unsigned heads = __ballot_sync(kFull, head);
+                        const unsigned after = heads & ~((2u << lane) - 1u);  // heads above this lane
+                        const int last = after ? __ffs(after) - 2 : 31;        // last lane of my run
+#pragma unroll
+                        for (int d = 1; d < 32; d <<= 1) {
+                            const T ox = __shfl_down_sync(kFull, gjx, d);
+                            const T oy = __shfl_down_sync(kFull, gjy, d);
+                            const T oz = __shfl_down_sync(kFull, gjz, d);
+                            if (lane + d <= last) {
+                                gjx += ox;
+                                gjy += oy;
+                                gjz += oz;
+                            }
+                        }
+                        if (head && lane < n) {
+                            atomicAdd(&s.g[pj].x, gjx);
+                            atomicAdd(&s.g[pj].y, gjy);
+                            atomicAdd(&s.g[pj].z, gjz);
+                        }
                     }
                     __syncwarp();
                     const int rem = qlen - n;
@@ -726,57 +806,67 @@ void set_smem(K kernel, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+// Shared memory per warp grows with the largest neighbour count of the
+// batch, and it sets how many warps an SM holds.  Atoms with at most
+// kSplitCount neighbours (about 98 % in the dense workloads) run in a launch
+// sized for that count; the rest follow in a second launch sized for the
+// batch maximum.  Each atom is evaluated once, by the same code.
+constexpr int kSplitCount = 64;
+
 template <typename T, class S>
-void run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
-    const int mm = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
-    const size_t smem = fast_warp_bytes<T>(mm, m.nsf_max, m.nblk, S::P, grad) * kWarps;
-    int blocks = (b.natoms + kWarps - 1) / kWarps;
-    const int cap = nsm() * 32;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    if (grad) {
-        set_smem(k_sfg_fast<T, S>, smem);
-        k_sfg_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+int run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
+    const int mfull = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
+    int L = 0;
+    auto go = [&](int mm, int mlo, int last) {
+        const size_t smem = fast_warp_bytes<T>(mm, m.g2max, m.nblk, S::P, grad) * kWarps;
+        int blocks = (b.natoms + kWarps - 1) / kWarps;
+        const int cap = nsm() * 32;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) blocks = 1;
+        if (grad) {
+            set_smem(k_sfg_fast<T, S>, smem);
+            k_sfg_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm, mlo, last);
+        } else {
+            set_smem(k_sfv_fast<T, S>, smem);
+            k_sfv_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm, mlo, last);
+        }
+        ++L;
+    };
+    if (mfull > kSplitCount) {
+        go(kSplitCount, -1, 0);
+        go(mfull, kSplitCount, 1);
     } else {
-        set_smem(k_sfv_fast<T, S>, smem);
-        k_sfv_fast<T, S><<<blocks, 32 * kWarps, smem, st>>>(b, m, mm);
+        go(mfull, -1, 1);
     }
+    return L;
 }
 
 template <typename T>
-void run_any(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
+int run_any(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
     switch (m.fast) {
-        case 1: run_spec<T, Spec<2, 2, 1>>(b, m, grad, st); break;
-        case 2: run_spec<T, Spec<2, 4, 2>>(b, m, grad, st); break;
-        case 3: run_spec<T, Spec<2, 4, 4>>(b, m, grad, st); break;
-        case 4: run_spec<T, Spec<2, 8, 2>>(b, m, grad, st); break;
-        case 5: run_spec<T, Spec<2, 2, 1, 1, 4>>(b, m, grad, st); break;
-        case 6: run_spec<T, Spec<2, 4, 2, 1, 2, 4, 16>>(b, m, grad, st); break;
-        default: break;
+        case 1: return run_spec<T, Spec<2, 2, 1>>(b, m, grad, st);
+        case 2: return run_spec<T, Spec<2, 4, 2>>(b, m, grad, st);
+        case 3: return run_spec<T, Spec<2, 4, 4>>(b, m, grad, st);
+        case 4: return run_spec<T, Spec<2, 8, 2>>(b, m, grad, st);
+        case 5: return run_spec<T, Spec<2, 2, 1, 1, 4>>(b, m, grad, st);
+        case 6: return run_spec<T, Spec<2, 4, 2, 1, 2, 4, 16>>(b, m, grad, st);
+        default: return 0;
     }
 }
 
 }  // namespace
 
-size_t sf_fast_smem_per_warp(int mmax, int nsf, int nblk, int P, bool grad, bool fp32) {
+size_t sf_fast_smem_per_warp(int mmax, int g2max, int nblk, int P, bool grad, bool fp32) {
     const int mm = mmax > 0 ? ((mmax + 31) / 32) * 32 : 32;
-    return fp32 ? fast_warp_bytes<float>(mm, nsf, nblk, P, grad) : fast_warp_bytes<double>(mm, nsf, nblk, P, grad);
+    return fp32 ? fast_warp_bytes<float>(mm, g2max, nblk, P, grad) : fast_warp_bytes<double>(mm, g2max, nblk, P, grad);
 }
 
 int launch_sf_values_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t st) {
-    if (fp32)
-        run_any<float>(b, m, false, st);
-    else
-        run_any<double>(b, m, false, st);
-    return 1;
+    return fp32 ? run_any<float>(b, m, false, st) : run_any<double>(b, m, false, st);
 }
 
 int launch_sf_gradients_fast(const Batch& b, const DevModel& m, bool fp32, cudaStream_t st) {
-    if (fp32)
-        run_any<float>(b, m, true, st);
-    else
-        run_any<double>(b, m, true, st);
-    return 1;
+    return fp32 ? run_any<float>(b, m, true, st) : run_any<double>(b, m, true, st);
 }
 
 }  // namespace hdnnp
