@@ -185,6 +185,8 @@ struct hdnnp_ctx {
     DevBuf<double> pos, wpos, G, dEdG, atE, gent, gself, vir, force, energy, dEdLat;
     DevBuf<float> Gf, dEdGf, atEf, gentf, gselff, virf;  // mixed-precision intermediates
     DevBuf<double> cm_acc, cm_E, cm_std;                  // committee: dE/dG sum, member energies, std
+    DevBuf<unsigned> pairs;                               // contributing-pair lists (fast kernels)
+    DevBuf<int> npairs;
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -207,6 +209,8 @@ struct hdnnp_ctx {
         for (auto* b : {&Gf, &dEdGf, &atEf, &gentf, &gselff, &virf}) b->release();
         info.release();
         stats.release();
+        pairs.release();
+        npairs.release();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
@@ -664,6 +668,12 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     // outside their shapes evaluate in FP64 with the generic kernels
     const bool fast = D.fast && !c->generic_sf;
     const bool mixed = c->precision == HDNNP_PREC_MIXED && fast;
+    if (fast) {
+        if ((r = c->pairs.ensure(N * (size_t)kPairCap)) || (r = c->npairs.ensure(N))) return r;
+        b.pairs = c->pairs.p;
+        b.npairs = c->npairs.p;
+        b.pcap = kPairCap;
+    }
     if (mixed) {
         if ((r = c->Gf.ensure(N * D.nsf_max)) || (r = c->dEdGf.ensure(N * D.nsf_max)) || (r = c->atEf.ensure(N)) ||
             (r = c->gentf.ensure(3 * E + 3)) || (r = c->gselff.ensure(3 * N)) || (r = c->virf.ensure(9 * N)))

@@ -165,7 +165,16 @@ struct Batch {
     const int* rebuild;
     double* wshift;
     double* pos_ref;
+    // Contributing angular pairs of each atom, written by the fast value pass
+    // (j | k << 10 | element-pair block << 20, enumeration order) and read by
+    // the gradient pass instead of screening the candidates again; atoms with
+    // more than pcap pairs are screened again.  Null: no list.
+    unsigned* pairs;          // [natoms * pcap]
+    int* npairs;              // [natoms]
+    int pcap;
 };
+
+constexpr int kPairCap = 1024;  // listed pairs per atom (the dense workloads average ~550)
 
 // Resident-plan mode of the pipeline (plan.cu): capacities fixed in advance
 // so that an evaluation needs no host read and can be captured in a CUDA

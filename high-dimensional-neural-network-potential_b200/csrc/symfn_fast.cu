@@ -471,6 +471,12 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 }
                 const unsigned bal = __ballot_sync(kFull, ok);
                 if (ok) s.queue[qlen + __popc(bal & lanemask_lt())] = (unsigned)j | ((unsigned)k << 16);
+                if (ok && b.pairs) {
+                    // contributing-pair list for the gradient pass (enumeration order)
+                    const long long slot = (long long)n_pairs + __popc(bal & lanemask_lt());
+                    if (slot < b.pcap)
+                        b.pairs[(size_t)i * b.pcap + slot] = (unsigned)j | ((unsigned)k << 10) | ((unsigned)t << 20);
+                }
                 qlen += __popc(bal);
                 n_pairs += __popc(bal);
                 __syncwarp();
@@ -538,6 +544,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 }
             }
         }
+        if (b.pairs && lane == 0) b.npairs[i] = n_pairs > (unsigned long long)INT32_MAX ? INT32_MAX : (int)n_pairs;
         if (b.stats && lane == 0) {
             unsigned long long n2 = 0;
             for (int f = r0; f < r1; ++f) n2 += s.est[m.g2[f].nel + 1] - s.est[m.g2[f].nel];
@@ -552,6 +559,109 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
 }
 
 // ---------------------------------------------------------------- pass 2
+// Gradient contributions of up to 32 contributing pairs (one per lane; pk =
+// j | k << 10 | block << 20, live for lane < n): dE/dr_k added to slot k,
+// dE/dr_j summed over runs of equal j (lanes hold pairs in enumeration order,
+// so equal j are contiguous) and added once per run.  Called by all lanes.
+template <typename T, class S>
+__device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m, int ne, T rc, T inv_rc, double rc2d,
+                                           unsigned pk_in, int n, int lane) {
+    constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
+        // dE/dr_j of this lane's pair, summed over runs of equal j below
+        int pj = -1 - lane;
+        T gjx = (T)0, gjy = (T)0, gjz = (T)0;
+        if (lane < n) {
+            const unsigned pk = pk_in;
+            pj = pk & 0x3ff;
+            const int pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
+            const V4<T> a = s.nb[pj], bq = s.nb[pq];
+            const V4<T> xa = s.ax[pj], xb = s.ax[pq];
+            const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
+            const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;  // djk = r_j - r_k
+            const T rjk2 = cx * cx + cy * cy + cz * cz;
+            const T rjk = xsqrt(rjk2);
+            const T irjk = (T)1 / rjk;
+            const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk)), tt = tj * tj;
+            const T fjk = tt * tj;
+            const T dfjk = (T)(-3) * inv_rc * irjk * (tt - tt * tt);
+            const T irj = xa.z, irk = xb.z;
+            const T t1 = -irj * irk;
+            const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
+            const T dot = a.x * bq.x + a.y * bq.y + a.z * bq.z;
+            const T cj = dot * irj * irj * irj * irk, ck = dot * irk * irk * irk * irj;
+            const T fcp = fj * fk * fjk;
+            const T R = a.w * a.w + bq.w * bq.w + rjk2;
+            T Y[NE];
+#pragma unroll
+            for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) : (T)0;
+            T SA[NE], SC[NE];
+#pragma unroll
+            for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
+            T wa[P], wc[P];
+            ldvec<P>(s.WA + pt * P, wa);
+            ldvec<P>(s.WC + pt * P, wc);
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                T Tz[NZ], Tp[NZ];
+                powers<S, true>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+#pragma unroll
+                for (int z = 0; z < NZ; ++z)
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) {
+                        SA[e] += wa[(l * NZ + z) * NE + e] * Tz[z];
+                        SC[e] += wc[(l * NZ + z) * NE + e] * Tp[z];
+                    }
+            }
+            T A = (T)0, B = (T)0, C = (T)0;
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                A += Y[e] * SA[e];
+                B += (T)m.eta4[e] * Y[e] * SA[e];
+                C += Y[e] * SC[e];
+            }
+            const T B2 = (T)2 * B * fcp, Cf = C * fcp;
+            const T pj1 = A * fk * fj * dfjk, pj2 = A * fk * dfj * fjk;
+            const T pk1 = A * fj * fk * dfjk, pk2 = A * fj * dfk * fjk;
+            gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
+            gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
+            gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
+            const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
+            const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
+            const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
+            atomicAdd(&s.g[pq].x, gkx);
+            atomicAdd(&s.g[pq].y, gky);
+            atomicAdd(&s.g[pq].z, gkz);
+        }
+        // Queue order is enumeration order, so pairs sharing j sit in
+        // contiguous lanes: a segmented suffix sum (fixed shuffle order)
+        // leaves each run's total in its first lane, which alone
+        // updates slot j -- instead of one conflicting atomic per lane.
+        {
+            // every lane executes the shuffle (no short-circuit around it)
+            const int prev_j = __shfl_up_sync(kFull, pj, 1);
+            const bool head = lane == 0 || prev_j != pj;
+            const unsigned heads = __ballot_sync(kFull, head);
+            const unsigned after = heads & ~((2u << lane) - 1u);  // heads above this lane
+            const int last = after ? __ffs(after) - 2 : 31;        // last lane of my run
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const T ox = __shfl_down_sync(kFull, gjx, d);
+                const T oy = __shfl_down_sync(kFull, gjy, d);
+                const T oz = __shfl_down_sync(kFull, gjz, d);
+                if (lane + d <= last) {
+                    gjx += ox;
+                    gjy += oy;
+                    gjz += oz;
+                }
+            }
+            if (head && lane < n) {
+                atomicAdd(&s.g[pj].x, gjx);
+                atomicAdd(&s.g[pj].y, gjy);
+                atomicAdd(&s.g[pj].z, gjz);
+            }
+        }
+}
+
 template <typename T, class S>
 __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fast(Batch b, DevModel m, int mm, int mlo, int last) {
     constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
@@ -619,7 +729,18 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
         }
         __syncwarp();
 
-        // angular: the queue spans element-pair blocks (entries carry the block)
+        // angular: the contributing pairs listed by the value pass, or (list
+        // missing or over capacity) screened again; the queue spans element-pair
+        // blocks (entries carry the block)
+        const int np = b.pairs ? b.npairs[i] : -1;
+        if (np >= 0 && np <= b.pcap) {
+            const unsigned* pl = b.pairs + (size_t)i * b.pcap;
+            for (int base = 0; base < np; base += 32) {
+                const int n = np - base < 32 ? np - base : 32;
+                grad_pairs<T, S>(s, m, ne, rc, inv_rc, rc2d, lane < n ? pl[base + lane] : 0u, n, lane);
+                __syncwarp();
+            }
+        } else {
         int qlen = 0;
         for (int t = 0; t < m.nblk; ++t) {
             const int gb = m.g4_off[c * m.nblk + t], ge = m.g4_off[c * m.nblk + t + 1];
@@ -648,99 +769,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
                 const bool flush_all = last_blk && cb + 32 >= ncand;
                 while (qlen >= 32 || (flush_all && qlen > 0)) {
                     const int n = qlen < 32 ? qlen : 32;
-                    // dE/dr_j of this lane's pair, summed over runs of equal j below
-                    int pj = -1 - lane;
-                    T gjx = (T)0, gjy = (T)0, gjz = (T)0;
-                    if (lane < n) {
-                        const unsigned pk = s.queue[lane];
-                        pj = pk & 0x3ff;
-                        const int pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
-                        const V4<T> a = s.nb[pj], bq = s.nb[pq];
-                        const V4<T> xa = s.ax[pj], xb = s.ax[pq];
-                        const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
-                        const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;  // djk = r_j - r_k
-                        const T rjk2 = cx * cx + cy * cy + cz * cz;
-                        const T rjk = xsqrt(rjk2);
-                        const T irjk = (T)1 / rjk;
-                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk)), tt = tj * tj;
-                        const T fjk = tt * tj;
-                        const T dfjk = (T)(-3) * inv_rc * irjk * (tt - tt * tt);
-                        const T irj = xa.z, irk = xb.z;
-                        const T t1 = -irj * irk;
-                        const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
-                        const T dot = a.x * bq.x + a.y * bq.y + a.z * bq.z;
-                        const T cj = dot * irj * irj * irj * irk, ck = dot * irk * irk * irk * irj;
-                        const T fcp = fj * fk * fjk;
-                        const T R = a.w * a.w + bq.w * bq.w + rjk2;
-                        T Y[NE];
-#pragma unroll
-                        for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) : (T)0;
-                        T SA[NE], SC[NE];
-#pragma unroll
-                        for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
-                        T wa[P], wc[P];
-                        ldvec<P>(s.WA + pt * P, wa);
-                        ldvec<P>(s.WC + pt * P, wc);
-#pragma unroll
-                        for (int l = 0; l < NL; ++l) {
-                            T Tz[NZ], Tp[NZ];
-                            powers<S, true>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
-#pragma unroll
-                            for (int z = 0; z < NZ; ++z)
-#pragma unroll
-                                for (int e = 0; e < NE; ++e) {
-                                    SA[e] += wa[(l * NZ + z) * NE + e] * Tz[z];
-                                    SC[e] += wc[(l * NZ + z) * NE + e] * Tp[z];
-                                }
-                        }
-                        T A = (T)0, B = (T)0, C = (T)0;
-#pragma unroll
-                        for (int e = 0; e < NE; ++e) {
-                            A += Y[e] * SA[e];
-                            B += (T)m.eta4[e] * Y[e] * SA[e];
-                            C += Y[e] * SC[e];
-                        }
-                        const T B2 = (T)2 * B * fcp, Cf = C * fcp;
-                        const T pj1 = A * fk * fj * dfjk, pj2 = A * fk * dfj * fjk;
-                        const T pk1 = A * fj * fk * dfjk, pk2 = A * fj * dfk * fjk;
-                        gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
-                        gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
-                        gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
-                        const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
-                        const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
-                        const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
-                        atomicAdd(&s.g[pq].x, gkx);
-                        atomicAdd(&s.g[pq].y, gky);
-                        atomicAdd(&s.g[pq].z, gkz);
-                    }
-                    // Queue order is enumeration order, so pairs sharing j sit in
-                    // contiguous lanes: a segmented suffix sum (fixed shuffle order)
-                    // leaves each run's total in its first lane, which alone
-                    // updates slot j -- instead of one conflicting atomic per lane.
-                    {
-                        // every lane executes the shuffle (no short-circuit around it)
-                        const int prev_j = __shfl_up_sync(kFull, pj, 1);
-                        const bool head = lane == 0 || prev_j != pj;
-                        const unsigned heads = __ballot_sync(kFull, head);
-                        const unsigned after = heads & ~((2u << lane) - 1u);  // heads above this lane
-                        const int last = after ? __ffs(after) - 2 : 31;        // last lane of my run
-#pragma unroll
-                        for (int d = 1; d < 32; d <<= 1) {
-                            const T ox = __shfl_down_sync(kFull, gjx, d);
-                            const T oy = __shfl_down_sync(kFull, gjy, d);
-                            const T oz = __shfl_down_sync(kFull, gjz, d);
-                            if (lane + d <= last) {
-                                gjx += ox;
-                                gjy += oy;
-                                gjz += oz;
-                            }
-                        }
-                        if (head && lane < n) {
-                            atomicAdd(&s.g[pj].x, gjx);
-                            atomicAdd(&s.g[pj].y, gjy);
-                            atomicAdd(&s.g[pj].z, gjz);
-                        }
-                    }
+                    grad_pairs<T, S>(s, m, ne, rc, inv_rc, rc2d, lane < n ? s.queue[lane] : 0u, n, lane);
                     __syncwarp();
                     const int rem = qlen - n;
                     unsigned v = 0;
@@ -751,6 +780,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
                     qlen = rem;
                 }
             }
+        }
         }
         __syncwarp();
         T* gent = Buf<T>::gent(b);
