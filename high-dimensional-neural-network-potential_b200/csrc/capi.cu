@@ -407,10 +407,13 @@ int upload_model(hdnnp_model* m) {
         off += (std::max<size_t>(bytes, 8) + 255) & ~size_t(255);
         return o;
     };
+    std::vector<double> sinvw(swidth.size());
+    for (size_t q = 0; q < swidth.size(); ++q) sinvw[q] = 1.0 / swidth[q];
     size_t o_rc = add(rc.data(), rc.size() * 8), o_nsf = add(nsf.data(), nsf.size() * 4),
            o_g2o = add(g2_off.data(), g2_off.size() * 4), o_g2 = add(g2.data(), g2.size() * sizeof(SF2)),
            o_g4o = add(g4_off.data(), g4_off.size() * 4), o_g4 = add(g4.data(), g4.size() * sizeof(SF4)),
            o_sm = add(smean.data(), smean.size() * 8), o_sw = add(swidth.data(), swidth.size() * 8),
+           o_siw = add(sinvw.data(), sinvw.size() * 8),
            o_w = add(w.data(), w.size() * 8), o_wt = add(wt.data(), wt.size() * 8), o_b = add(bias.data(), bias.size() * 8),
            o_wo = add(w_off.data(), w_off.size() * 8), o_bo = add(b_off.data(), b_off.size() * 8),
            o_ae = add(ae.data(), ae.size() * 8);
@@ -492,6 +495,7 @@ int upload_model(hdnnp_model* m) {
     D.g4 = (const SF4*)(base + o_g4);
     D.smean = (const double*)(base + o_sm);
     D.swidth = (const double*)(base + o_sw);
+    D.sinvw = (const double*)(base + o_siw);
     D.w = (const double*)(base + o_w);
     D.wt = (const double*)(base + o_wt);
     D.b = (const double*)(base + o_b);

@@ -68,6 +68,7 @@ struct DevModel {
     const SF4* g4;
     const double* smean;      // [nel*nsf_max] (0 when not centring)
     const double* swidth;     // [nel*nsf_max] (1 when not scaling)
+    const double* sinvw;      // [nel*nsf_max] 1 / swidth (fast kernels multiply)
     // networks
     int nlayers;
     int width[9];             // width[0] = input (per element: nsf), width[l+1] = out of layer l

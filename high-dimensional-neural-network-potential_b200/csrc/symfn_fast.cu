@@ -240,18 +240,20 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
         }
         __syncwarp();
         if (keep) {
+            // distance and cutoff in FP64 (one division)
             const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            const double ir = 1.0 / r, irc = 1.0 / rc;
             double fc = 0.0, dfc = 0.0;
             if (r < rc) {
-                const double t = tanh(1.0 - r / rc), tt = t * t;
+                const double t = tanh(1.0 - r * irc), tt = t * t;
                 fc = tt * t;
-                dfc = -3.0 / (rc * r) * (tt - tt * tt);
+                dfc = -3.0 * irc * ir * (tt - tt * tt);
             }
             s.nb[slot] = V4<T>{(T)dx, (T)dy, (T)dz, (T)r};
             if (sizeof(T) == 4)
                 s.lo[slot] = V4<float>{(float)(dx - (double)(float)dx), (float)(dy - (double)(float)dy),
                                        (float)(dz - (double)(float)dz), 0.0f};
-            s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)(1.0 / r), (T)0};
+            s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)ir, (T)0};
             s.el[slot] = (unsigned char)el;
             if (kGrad) {
                 s.g[slot] = V4<T>{(T)0, (T)0, (T)0, (T)0};
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         const double rc2d = m.rc[c] * m.rc[c];
         T* Gi = Gout + (size_t)i * m.nsf_max;
         const double* mean = m.smean + (size_t)c * m.nsf_max;
-        const double* width = m.swidth + (size_t)c * m.nsf_max;
+        const double* iwidth = m.sinvw + (size_t)c * m.nsf_max;
 
         // radial SFs: lane = SF
         const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 const T x = s.nb[t].w - rs;
                 acc += xexp(-eta * x * x) * s.ax[t].x;
             }
-            Gi[q.sf] = (T)(((double)acc - mean[q.sf]) / width[q.sf]);
+            Gi[q.sf] = (T)(((double)acc - mean[q.sf]) * iwidth[q.sf]);
         }
 
         unsigned long long n_cand = 0, n_pairs = 0;
@@ -540,7 +542,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 const int sf = m.pmap[((size_t)c * m.nblk + t) * P + lane];
                 if (sf >= 0) {
                     const int z = (lane / NE) % NZ;
-                    Gi[sf] = (T)(((double)((T)m.pfz[z] * sum) - mean[sf]) / width[sf]);
+                    Gi[sf] = (T)(((double)((T)m.pfz[z] * sum) - mean[sf]) * iwidth[sf]);
                 }
             }
         }
@@ -688,11 +690,11 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
         // w_s = dE/dG_s / width_s: radial SFs staged per slot of g2, angular
         // ones folded into the product-space weight tensors of each block
         const T* dEdGi = dEdG + (size_t)i * m.nsf_max;
-        const double* widc = m.swidth + (size_t)c * m.nsf_max;
+        const double* iwc = m.sinvw + (size_t)c * m.nsf_max;
         const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
         for (int f = r0 + lane; f < r1; f += 32) {
             const int sf = m.g2[f].sf;
-            s.w2[f - r0] = (T)((double)dEdGi[sf] / widc[sf]);
+            s.w2[f - r0] = (T)((double)dEdGi[sf] * iwc[sf]);
         }
         for (int q = lane; q < m.nblk * P; q += 32) {
             const int t = q / P, p = q % P;
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
             T wa = (T)0, wc = (T)0;
             if (sf >= 0) {
                 const int l = p / (NZ * NE), z = (p / NE) % NZ;
-                wa = (T)((double)dEdGi[sf] / widc[sf]) * (T)m.pfz[z];
+                wa = (T)((double)dEdGi[sf] * iwc[sf]) * (T)m.pfz[z];
                 wc = wa * (T)m.lam[l] * (T)m.zet[z];
             }
             s.WA[q] = wa;
