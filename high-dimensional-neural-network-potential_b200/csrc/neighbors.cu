@@ -192,24 +192,34 @@ __global__ void k_reverse(Batch b) {
     const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (a >= b.natoms || keep_list(b)) return;  // uniform per warp
+    // four entries of atom a at a time, one per group of 8 lanes, so that the
+    // dependent loads of four searches overlap
+    const int grp = lane >> 3, gl = lane & 7;
     const int e1 = b.nei_off[a + 1];
-    for (int e = b.nei_off[a]; e < e1; ++e) {
-        const int j = b.nei_j[e];
-        int sx, sy, sz;
-        unpack_shift(b.nei_s[e], sx, sy, sz);
-        const int want = pack_shift(-sx, -sy, -sz);
-        const int f1 = b.nei_off[j + 1];
-        int r = -1;
-        for (int fb = b.nei_off[j]; fb < f1; fb += 32) {
-            const int f = fb + lane;
-            const bool hit = f < f1 && b.nei_j[f] == a && b.nei_s[f] == want;
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (m) {
-                r = fb + __ffs(m) - 1;
-                break;
-            }
+    for (int e0 = b.nei_off[a]; e0 < e1; e0 += 4) {
+        const int e = e0 + grp;
+        const bool live = e < e1;
+        int want = 0, f0 = 0, f1 = 0;
+        if (live) {
+            const int j = b.nei_j[e];
+            int sx, sy, sz;
+            unpack_shift(b.nei_s[e], sx, sy, sz);
+            want = pack_shift(-sx, -sy, -sz);
+            f0 = b.nei_off[j];
+            f1 = b.nei_off[j + 1];
         }
-        if (lane == 0) {
+        int r = -1;
+        // every iteration advances each open search by 8 entries of its list,
+        // so the loop ends after (longest list) / 8 iterations
+        for (int fb = 0;; fb += 8) {
+            const int f = f0 + fb + gl;
+            const bool open = live && r < 0 && f0 + fb < f1;
+            const bool hit = open && f < f1 && b.nei_j[f] == a && b.nei_s[f] == want;
+            const unsigned gm = (__ballot_sync(0xffffffffu, hit) >> (8 * grp)) & 0xffu;
+            if (open && gm) r = f0 + fb + __ffs(gm) - 1;
+            if (!__any_sync(0xffffffffu, live && r < 0 && f0 + fb + 8 < f1)) break;
+        }
+        if (live && gl == 0) {
             if (r < 0) atomicOr(&b.status[0], 2);  // asymmetric list (should not happen)
             b.nei_rev[e] = r < 0 ? e : r;
         }
