@@ -11,14 +11,18 @@ and N(0, 0.15 Bohr) jitter (seed 4 + rank), synthetic 5-element potential with
   python bench.py --impl reference ...   # the reference's algorithm on the host cores
 
 value  = atoms x steps / device time of the K steps (max over ranks), inputs
-         resident in HBM, batched path (hdnnp_eval_batch_device), default
-         precision "mixed" (FP32 symmetry functions and networks, FP64 wrap,
-         energy and virial reductions).
+         resident in HBM, the batch as a resident plan (hdnnp_plan_*: one
+         CUDA-graph launch per step, autotuned symmetry-function launches),
+         default precision "mixed" (FP32 symmetry functions, tensor-core
+         networks, FP64 wrap, energy and virial reductions).
 e2e    = the same through hdnnp_eval_batch with pinned host buffers: H2D of
          Z/positions and D2H of energies/forces/dE/dh inside every step.
-config.compare: the batched FP64 path (same workload) and the plain FP64 form
-         (hdnnp_energy_and_forces, one structure per call, the reference's API)
-         on a sample of the structures, for the north-star ratio.
+config.compare: the eager batched path (hdnnp_eval_batch_device), the
+         batched FP64 plan, the plain FP64 form (hdnnp_energy_and_forces, one
+         structure per call, the reference's API) on a sample of the
+         structures for the north-star ratio, the served walkers, and the
+         single-structure legs (methylammonium MD, 768-atom cell, 49,152-atom
+         MD) with the CPU stand-in beside each.
 """
 from __future__ import annotations
 
@@ -417,7 +421,8 @@ def main():
     # the batch as a resident plan: one CUDA-graph launch per step, no host work
     from hdnnp_b200 import plan as PLm
 
-    bplan = PLm.Plan(pot, structs, precision=prec, margin=0.02, profile=True)
+    # autotuned launch shape of the symmetry-function kernels (before timing)
+    bplan = PLm.Plan(pot, structs, precision=prec, margin=0.02, profile=True, autotune=True)
 
     def step_device():
         bplan.launch(stream.cuda_stream)
@@ -571,6 +576,7 @@ def main():
                                        f"(12-768 atoms, {natoms} atoms, seed 4+rank), E+F+stress",
                            "global_batch": natoms * world, "precision": args.precision,
                            "parallelism": f"replicas x{world} (independent structures per GPU)",
+                           "autotuned": bplan.tuning(),
                            "l2": "256 MB buffer written between timed steps; working set (G alone "
                                  f"{natoms * 280 * 4 / 1e9:.1f}+ GB) is larger than L2",
                            "compare": compare},

@@ -177,6 +177,8 @@ struct hdnnp_ctx {
     int generic_sf = 0;
     int runtime_zeta = 0;
     int mlp_simt = 0;
+    int sf_split = 0;          // launch shape of the fast SF kernels (0: defaults)
+    int sf_blocks_per_sm = 0;
     int launches = 0;
     // device buffers
     DevBuf<StructInfo> info;
@@ -597,6 +599,8 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.force = force_d;
     b.energy = energy_d;
     b.dEdLat = dEdLat_d;
+    b.sf_split = c->sf_split;
+    b.sf_blocks_per_sm = c->sf_blocks_per_sm;
     b.rc_list = pp ? pp->rc_list : 0.0;
     b.rebuild = pp ? pp->rebuild : nullptr;
     b.wshift = pp ? pp->wshift : nullptr;
@@ -843,6 +847,16 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
     }
     if (std::string(name) == "runtime_zeta") {
         c->runtime_zeta = value != 0;
+        return HDNNP_OK;
+    }
+    if (std::string(name) == "sf_split") {
+        if (value < -1 || value > 1024) return fail(HDNNP_E_INPUT, "sf_split must be -1, 0 or 1..1024");
+        c->sf_split = value;
+        return HDNNP_OK;
+    }
+    if (std::string(name) == "sf_blocks_per_sm") {
+        if (value < 0 || value > 64) return fail(HDNNP_E_INPUT, "sf_blocks_per_sm must be 0..64");
+        c->sf_blocks_per_sm = value;
         return HDNNP_OK;
     }
     return fail(HDNNP_E_INPUT, std::string("unknown option ") + name);

@@ -173,6 +173,11 @@ struct Batch {
     unsigned* pairs;          // [natoms * pcap]
     int* npairs;              // [natoms]
     int pcap;
+    // Launch shape of the fast symmetry-function kernels (0: defaults): the
+    // neighbour count splitting the two launches (-1: one launch) and the
+    // persistent grid in blocks per SM.  Set by the plans' autotuner.
+    int sf_split;
+    int sf_blocks_per_sm;
 };
 
 constexpr int kPairCap = 1024;  // listed pairs per atom (the dense workloads average ~550)

@@ -91,6 +91,9 @@ struct hdnnp_plan {
     cudaGraphExec_t exec = nullptr;
     long long launches = 0, launches_synced = 0;
     int kernels_per_launch = 0;
+    // autotuner result (launch shape of the symmetry-function kernels)
+    int tuned_split = 0, tuned_per_sm = 0;
+    double tuned_ms = 0.0;
 };
 
 namespace {
@@ -130,6 +133,50 @@ int plan_body(hdnnp_plan* p, cudaStream_t st) {
         L += r + 2;
     }
     return L;
+}
+
+// Autotuner: times the two symmetry-function stages (values + gradients) of
+// the plan's own batch on its stream for each candidate launch shape -- the
+// neighbour count that splits the two launches (or one launch) and the
+// persistent grid in blocks per SM -- and keeps the fastest.  Each candidate
+// runs twice, the second run is timed with the stage events.
+int plan_autotune(hdnnp_plan* p) {
+    static const int kSplits[] = {-1, 32, 48, 64, 96};
+    static const int kPerSm[] = {8, 16, 32};
+    hdnnp_ctx* c = p->ctx;
+    int r = hdnnp_ctx_set_profiling(c, 1);
+    double best = 1e300;
+    int bs = 0, bp = 0;
+    for (int sp : kSplits) {
+        if (sp > 0 && sp >= p->pp.m_cap) continue;  // same as one launch
+        for (int ps : kPerSm) {
+            if ((r = hdnnp_ctx_set_option(c, "sf_split", sp)) || (r = hdnnp_ctx_set_option(c, "sf_blocks_per_sm", ps)))
+                return r;
+            double ms[8] = {0};
+            for (int rep = 0; rep < 2; ++rep) {
+                if ((r = hdnnp_profile_read(c, nullptr, nullptr, 1))) return r;
+                const int L = plan_eval(p, p->stream);
+                if (L < 0) return -L;
+                if (cudaStreamSynchronize(p->stream) != cudaSuccess) return set_error(HDNNP_E_CUDA, "autotune run failed");
+                if ((r = ctx_profile_replay(c, 1, p->natoms))) return r;
+            }
+            if ((r = hdnnp_profile_read(c, ms, nullptr, 1))) return r;
+            const double t = ms[3] + ms[5];
+            if (t < best) {
+                best = t;
+                bs = sp;
+                bp = ps;
+            }
+        }
+    }
+    if ((r = hdnnp_ctx_set_option(c, "sf_split", bs)) || (r = hdnnp_ctx_set_option(c, "sf_blocks_per_sm", bp)) ||
+        (r = hdnnp_ctx_set_profiling(c, p->o.profile ? 1 : 0)) || (r = hdnnp_profile_read(c, nullptr, nullptr, 1)))
+        return r;
+    p->tuned_split = bs;
+    p->tuned_per_sm = bp;
+    p->tuned_ms = best;
+    cudaMemset(p->acc, 0, 2 * sizeof(int));
+    return HDNNP_OK;
 }
 
 void plan_release(hdnnp_plan* p) {
@@ -221,6 +268,7 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
     }
     cudaMemset(p->acc, 0, 2 * sizeof(int));
     if (o->profile) hdnnp_profile_read(p->ctx, nullptr, nullptr, 1);  // the probe is not a launch
+    if (o->autotune && (r = plan_autotune(p))) return bail(r, hdnnp_last_error());
     // capture one launch
     p->pp.upload = false;
     if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
@@ -273,6 +321,14 @@ int hdnnp_plan_sync(hdnnp_plan* p, void* stream, int64_t* list_builds) {
 int hdnnp_plan_profile(hdnnp_plan* p, double* stage_ms, int64_t* counters, int reset) {
     if (!p) return set_error(HDNNP_E_INPUT, "null plan");
     return hdnnp_profile_read(p->ctx, stage_ms, counters, reset);
+}
+
+int hdnnp_plan_tuning(const hdnnp_plan* p, int* sf_split, int* sf_blocks_per_sm, double* sf_ms) {
+    if (!p) return set_error(HDNNP_E_INPUT, "null plan");
+    if (sf_split) *sf_split = p->tuned_split;
+    if (sf_blocks_per_sm) *sf_blocks_per_sm = p->tuned_per_sm;
+    if (sf_ms) *sf_ms = p->tuned_ms;
+    return HDNNP_OK;
 }
 
 int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_per_launch) {

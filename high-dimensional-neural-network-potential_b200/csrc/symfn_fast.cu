@@ -839,20 +839,25 @@ void set_smem(K kernel, size_t smem) {
 }
 
 // Shared memory per warp grows with the largest neighbour count of the
-// batch, and it sets how many warps an SM holds.  Atoms with at most
-// kSplitCount neighbours (about 98 % in the dense workloads) run in a launch
-// sized for that count; the rest follow in a second launch sized for the
-// batch maximum.  Each atom is evaluated once, by the same code.
+// batch, and it sets how many warps an SM holds.  Atoms with at most `split`
+// neighbours (64 by default: about 98 % in the dense workloads) run in a
+// launch sized for that count; the rest follow in a second launch sized for
+// the batch maximum.  Each atom is evaluated once, by the same code.  The
+// split and the persistent grid (blocks per SM) are the knobs of the plans'
+// autotuner (Batch::sf_split, Batch::sf_blocks_per_sm).
 constexpr int kSplitCount = 64;
+constexpr int kBlocksPerSm = 32;
 
 template <typename T, class S>
 int run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
     const int mfull = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
+    const int split = b.sf_split > 0 ? b.sf_split : b.sf_split < 0 ? mfull : kSplitCount;
+    const int per_sm = b.sf_blocks_per_sm > 0 ? b.sf_blocks_per_sm : kBlocksPerSm;
     int L = 0;
     auto go = [&](int mm, int mlo, int last) {
         const size_t smem = fast_warp_bytes<T>(mm, m.g2max, m.nblk, S::P, grad) * kWarps;
         int blocks = (b.natoms + kWarps - 1) / kWarps;
-        const int cap = nsm() * 32;
+        const int cap = nsm() * per_sm;
         if (blocks > cap) blocks = cap;
         if (blocks < 1) blocks = 1;
         if (grad) {
@@ -864,9 +869,9 @@ int run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
         }
         ++L;
     };
-    if (mfull > kSplitCount) {
-        go(kSplitCount, -1, 0);
-        go(mfull, kSplitCount, 1);
+    if (mfull > split) {
+        go(split, -1, 0);
+        go(mfull, split, 1);
     } else {
         go(mfull, -1, 1);
     }

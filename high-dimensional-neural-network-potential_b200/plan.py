@@ -26,7 +26,7 @@ from .engine import HDNNP_PREC_FP64, _check, lib
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("margin", C.c_double), ("skin", C.c_double), ("momenta_dev", C.c_void_p),
                 ("masses_dev", C.c_void_p), ("dt", C.c_double), ("steps_per_launch", C.c_int),
-                ("energy_hist_dev", C.c_void_p), ("profile", C.c_int)]
+                ("energy_hist_dev", C.c_void_p), ("profile", C.c_int), ("autotune", C.c_int)]
 
 
 def _register():
@@ -39,6 +39,7 @@ def _register():
     L.hdnnp_plan_sync.argtypes = [P, P, C.POINTER(C.c_int64)]
     L.hdnnp_plan_info.argtypes = [P, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.hdnnp_plan_profile.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+    L.hdnnp_plan_tuning.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.hdnnp_plan_free.argtypes = [P]
     L.hdnnp_plan_free.restype = None
     L._plan_registered = True
@@ -48,7 +49,7 @@ def _register():
 class Plan:
     def __init__(self, pot, structs, precision: int = HDNNP_PREC_FP64, margin: float = 0.25, skin: float = 0.0,
                  masses=None, momenta=None, dt: float = 0.0, steps_per_launch: int = 1, want_dEdLat: bool = True,
-                 profile: bool = False):
+                 profile: bool = False, autotune: bool = False):
         import torch
 
         L = _register()
@@ -74,7 +75,7 @@ class Plan:
             self.hist = torch.zeros(steps_per_launch, self.nstruct, dtype=torch.float64, device=dev)
         ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
         self._opts = _Opts(int(precision), float(margin), float(skin), ptr(self.mom), ptr(self.mass), float(dt),
-                           int(steps_per_launch), ptr(self.hist), 1 if profile else 0)
+                           int(steps_per_launch), ptr(self.hist), 1 if profile else 0, 1 if autotune else 0)
         self._per, self._lat = per, lat
         h = C.c_void_p()
         _check(L.hdnnp_plan_create(pot._m, C.byref(self._opts), self.nstruct, off.ctypes.data_as(C.c_void_p),
@@ -96,6 +97,12 @@ class Plan:
         k = C.c_int()
         _check(lib().hdnnp_plan_info(self._h, C.byref(e), C.byref(k)))
         return {"entry_capacity": e.value, "kernels_per_launch": k.value}
+
+    def tuning(self):
+        """Launch shape chosen by the autotuner and its symmetry-function time."""
+        a, b, t = C.c_int(), C.c_int(), C.c_double()
+        _check(lib().hdnnp_plan_tuning(self._h, C.byref(a), C.byref(b), C.byref(t)))
+        return {"sf_split": a.value, "sf_blocks_per_sm": b.value, "sf_ms": t.value}
 
     def profile(self, reset: bool = False):
         """(stage times in ms, work counters) as engine.Hdnnp.profile."""

@@ -77,7 +77,10 @@ int hdnnp_ctx_create(hdnnp_model* m, hdnnp_ctx** out);
 void hdnnp_ctx_free(hdnnp_ctx* c);
 int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
 
-/* Context options (for tests and tuning): "generic_sf" = 1 forces the
+/* Context options (for tests and tuning): "sf_split" (-1: one launch; 0:
+ * default 64; n: atoms with more than n neighbours in a second launch) and
+ * "sf_blocks_per_sm" (0: default 32) shape the launches of the
+ * lambda x zeta x eta kernels; "generic_sf" = 1 forces the
  * generic symmetry-function kernels (one parameter record per SF) instead of
  * the lambda x zeta x eta kernels; "runtime_zeta" = 1 makes the
  * lambda x zeta x eta kernels read the zeta set from the model even when a
@@ -217,6 +220,10 @@ typedef struct {
     int steps_per_launch;    /* MD steps per launch                                    */
     double* energy_hist_dev; /* NULL or steps_per_launch*nstruct energies per launch    */
     int profile;             /* 1: stage events captured in the graph (hdnnp_plan_profile) */
+    int autotune;            /* 1: before capture, time the symmetry-function kernels of this
+                                batch for each candidate launch shape (neighbour-count split
+                                of the two launches, persistent grid per SM) and keep the
+                                fastest (hdnnp_plan_tuning)                               */
 } hdnnp_plan_opts;
 
 int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* opts, int nstruct, const int64_t* atom_off,
@@ -233,6 +240,9 @@ int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_p
  * last evaluation of the last launch before each sync); the work counters
  * cover every evaluation.                                                     */
 int hdnnp_plan_profile(hdnnp_plan* p, double* stage_ms, int64_t* counters, int reset);
+/* Launch shape the autotuner chose (0, 0 without autotune: defaults) and the
+ * symmetry-function time it measured for it (ms per evaluation).           */
+int hdnnp_plan_tuning(const hdnnp_plan* p, int* sf_split, int* sf_blocks_per_sm, double* sf_ms);
 void hdnnp_plan_free(hdnnp_plan* p);
 
 /* ---------------------------------------------------------------- serving

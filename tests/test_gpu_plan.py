@@ -160,3 +160,24 @@ def test_capacity_overflow_is_flagged(pot, PL, W):
         p.sync()
         ref = pot.eval_batch([s], dEdLat=False)
         assert np.array_equal(p.results()[0], ref["energy"])
+
+
+def test_autotuned_plan_equals_eager(pot, PL, W):
+    """The autotuner only changes the launch shape of the symmetry-function
+    kernels; every shape gives bitwise the same FP64 result."""
+    structs = cells(W, [(2, 2, 2), (3, 2, 2), (1, 1, 2)], 13)
+    ref = pot.eval_batch(structs, dEdLat=True)
+    with PL.Plan(pot, structs, autotune=True) as p:
+        t = p.tuning()
+        assert t["sf_blocks_per_sm"] in (8, 16, 32) and t["sf_split"] in (-1, 32, 48, 64, 96) and t["sf_ms"] > 0
+        p.launch()
+        p.sync()
+        E, F, D = p.results()
+    assert np.array_equal(E, ref["energy"]) and np.array_equal(F, ref["forces"])
+    for split in (-1, 32, 96):
+        pot.set_option("sf_split", split)
+        pot.set_option("sf_blocks_per_sm", 8)
+        out = pot.eval_batch(structs, dEdLat=True)
+        assert np.array_equal(out["energy"], ref["energy"]) and np.array_equal(out["forces"], ref["forces"])
+    pot.set_option("sf_split", 0)
+    pot.set_option("sf_blocks_per_sm", 0)
