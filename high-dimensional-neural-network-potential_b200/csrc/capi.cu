@@ -1233,6 +1233,8 @@ namespace hdnnp {
 
 int model_device(const hdnnp_model* m) { return m->device; }
 
+const DevModel& model_devmodel(const hdnnp_model* m) { return m->dev; }
+
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 
 // Device-resident batch (as hdnnp_eval_batch_device) in which molecules are

@@ -210,6 +210,23 @@ struct Committee {
     double* std_dev;                 // device [nstruct] or null
 };
 
+// Single-block MD of one small molecule (fused_md.cu): every stage of
+// `nsteps` velocity-Verlet steps in one kernel launch.
+constexpr int kSmallMolecule = 64;  // atoms
+struct SmallMdArgs {
+    int natoms, nsteps;
+    double dt;
+    double* pos;
+    double* mom;
+    const double* mass;
+    double* force;
+    double* fprev;
+    double* energy;
+    double* hist;       // [nsteps] energies or null
+    int* acc;           // [2]: OR of status flags, evaluations
+    int el_start[kMaxEl + 1];  // atoms grouped by element in Batch::el_atoms
+};
+
 // packed image shift: three signed 8-bit lattice multiples
 __host__ __device__ inline int pack_shift(int x, int y, int z) {
     return (x & 0xff) | ((y & 0xff) << 8) | ((z & 0xff) << 16);
@@ -250,6 +267,8 @@ int launch_committee_finish(const Batch& b, const Committee& cm, const double* E
 size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
+size_t small_md_smem_bytes(const DevModel& m, int mm);
+int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& a, cudaStream_t s);
 
 // Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).
 // Ids 1-4 read zeta from the model; ids 5-6 have the zeta set compiled in

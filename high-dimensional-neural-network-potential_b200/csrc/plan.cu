@@ -35,6 +35,7 @@ int ctx_run_planned(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Z_dev,
                     double* energy_dev, double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan& pp);
 int* ctx_status_dev(hdnnp_ctx* c);
 int ctx_profile_replay(hdnnp_ctx* c, long long evals, long long atoms);
+const DevModel& model_devmodel(const hdnnp_model* m);
 }  // namespace hdnnp
 
 using namespace hdnnp;
@@ -94,6 +95,11 @@ struct hdnnp_plan {
     // autotuner result (launch shape of the symmetry-function kernels)
     int tuned_split = 0, tuned_per_sm = 0;
     double tuned_ms = 0.0;
+    // single-block MD of a small molecule (fused_md.cu) instead of the graph
+    bool small = false;
+    Batch sb{};
+    SmallMdArgs sa{};
+    void* sscratch = nullptr;
 };
 
 namespace {
@@ -179,6 +185,87 @@ int plan_autotune(hdnnp_plan* p) {
     return HDNNP_OK;
 }
 
+// Scratch and arguments of the single-block MD kernel: neighbour lists of up
+// to N*N entries, per-atom SF and network arrays, element groups (host-built
+// from Z; the kernel does not regroup).
+int plan_setup_small(hdnnp_plan* p) {
+    const DevModel& D = model_devmodel(p->model);
+    const int N = p->natoms;
+    std::vector<int32_t> Z((size_t)N);
+    if (cudaMemcpy(Z.data(), p->Z, sizeof(int32_t) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return set_error(HDNNP_E_CUDA, "reading Z failed");
+    std::vector<int> elem((size_t)N), grouped;
+    for (int i = 0; i < N; ++i) {
+        elem[i] = (Z[i] >= 1 && Z[i] <= 118) ? D.z2e[Z[i]] : -1;
+        if (elem[i] < 0) return set_error(HDNNP_E_INPUT, "atom with an element that is not in the potential");
+    }
+    for (int e = 0; e < D.nel; ++e) {
+        p->sa.el_start[e] = (int)grouped.size();
+        for (int i = 0; i < N; ++i)
+            if (elem[i] == e) grouped.push_back(i);
+    }
+    p->sa.el_start[D.nel] = (int)grouped.size();
+    // layout: doubles first, then StructInfo, then ints
+    const size_t NN = (size_t)N * N, nsf = (size_t)D.nsf_max;
+    const size_t nd = 2 * N * nsf + N + 3 * NN + 3 * N + 9 * N;
+    const size_t ni = (N + 1) + 3 * NN + 3 * N + 4;
+    const size_t bytes = nd * 8 + sizeof(StructInfo) + ni * 4;
+    if (cudaMalloc(&p->sscratch, bytes) != cudaSuccess) return set_error(HDNNP_E_CUDA, "small-MD scratch allocation");
+    double* d = (double*)p->sscratch;
+    StructInfo* info = (StructInfo*)(d + nd);
+    int* q = (int*)(info + 1);
+    Batch& b = p->sb;
+    b = Batch{};
+    b.nstruct = 1;
+    b.natoms = N;
+    b.G = d; d += N * nsf;
+    b.dEdG = d; d += N * nsf;
+    b.atE = d; d += N;
+    b.gent = d; d += 3 * NN;
+    b.gself = d; d += 3 * N;
+    b.vir = d;
+    b.info = info;
+    b.nei_off = q; q += N + 1;
+    b.nei_j = q; q += NN;
+    b.nei_s = q; q += NN;
+    b.nei_rev = q; q += NN;
+    b.elem = q; q += N;
+    b.sid = q; q += N;
+    b.el_atoms = q; q += N;
+    b.status = q;
+    b.Z = p->Z;
+    b.pos = p->pos;
+    b.wpos = p->pos;  // molecule: no wrap; relative vectors are differences of positions
+    b.force = p->F;
+    b.energy = p->E;
+    b.mmax = N - 1;
+    b.nentries = (int)NN;
+    StructInfo S{};
+    for (int k = 0; k < 9; ++k) S.h[k] = S.hinv[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    S.ngrid[0] = S.ngrid[1] = S.ngrid[2] = 1;
+    S.nat = N;
+    std::vector<int> zeros((size_t)N, 0);
+    if (cudaMemcpy(info, &S, sizeof S, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b.elem, elem.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b.sid, zeros.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b.el_atoms, grouped.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b.status, 0, 4 * sizeof(int)) != cudaSuccess)
+        return set_error(HDNNP_E_CUDA, "small-MD set-up copies failed");
+    SmallMdArgs& a = p->sa;
+    a.natoms = N;
+    a.nsteps = p->o.steps_per_launch;
+    a.dt = p->o.dt;
+    a.pos = p->pos;
+    a.mom = p->o.momenta_dev;
+    a.mass = p->o.masses_dev;
+    a.force = p->F;
+    a.fprev = p->fprev;
+    a.energy = p->E;
+    a.hist = p->o.energy_hist_dev;
+    a.acc = p->acc;
+    return HDNNP_OK;
+}
+
 void plan_release(hdnnp_plan* p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
@@ -186,6 +273,7 @@ void plan_release(hdnnp_plan* p) {
     for (void* q : {(void*)p->acc, (void*)p->rebuild, (void*)p->wshift, (void*)p->pos_ref, (void*)p->fprev})
         if (q) cudaFree(q);
     if (p->h_acc) cudaFreeHost(p->h_acc);
+    if (p->sscratch) cudaFree(p->sscratch);
     if (p->stream) cudaStreamDestroy(p->stream);
     if (p->ctx) hdnnp_ctx_free(p->ctx);
 }
@@ -269,6 +357,20 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
     cudaMemset(p->acc, 0, 2 * sizeof(int));
     if (o->profile) hdnnp_profile_read(p->ctx, nullptr, nullptr, 1);  // the probe is not a launch
     if (o->autotune && (r = plan_autotune(p))) return bail(r, hdnnp_last_error());
+    // one small molecule in FP64: every MD step of a launch in one kernel
+    {
+        const DevModel& D = model_devmodel(m);
+        const int mm = ((p->natoms - 1 + 31) / 32) * 32 < 32 ? 32 : ((p->natoms - 1 + 31) / 32) * 32;
+        p->small = o->momenta_dev && nstruct == 1 && !periodic[0] && p->natoms <= kSmallMolecule &&
+                   o->precision == HDNNP_PREC_FP64 && !o->profile && o->single_block >= 0 &&
+                   small_md_smem_bytes(D, mm) <= 200 * 1024;
+        if (p->small) {
+            if ((r = plan_setup_small(p))) return bail(r, hdnnp_last_error());
+            p->kernels_per_launch = 1;
+            *out = p;
+            return HDNNP_OK;
+        }
+    }
     // capture one launch
     p->pp.upload = false;
     if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
@@ -286,8 +388,15 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
 }
 
 int hdnnp_plan_launch(hdnnp_plan* p, void* stream) {
-    if (!p || !p->exec) return set_error(HDNNP_E_INPUT, "null plan");
+    if (!p || (!p->exec && !p->small)) return set_error(HDNNP_E_INPUT, "null plan");
     cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    if (p->small) {
+        launch_small_md(p->sb, model_devmodel(p->model), p->sa, st);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_error(HDNNP_E_CUDA, std::string("single-block MD: ") + cudaGetErrorString(e));
+        ++p->launches;
+        return HDNNP_OK;
+    }
     const cudaError_t e = cudaGraphLaunch(p->exec, st);
     if (e != cudaSuccess) return set_error(HDNNP_E_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
     ++p->launches;

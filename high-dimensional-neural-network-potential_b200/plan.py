@@ -26,7 +26,8 @@ from .engine import HDNNP_PREC_FP64, _check, lib
 class _Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("margin", C.c_double), ("skin", C.c_double), ("momenta_dev", C.c_void_p),
                 ("masses_dev", C.c_void_p), ("dt", C.c_double), ("steps_per_launch", C.c_int),
-                ("energy_hist_dev", C.c_void_p), ("profile", C.c_int), ("autotune", C.c_int)]
+                ("energy_hist_dev", C.c_void_p), ("profile", C.c_int), ("autotune", C.c_int),
+                ("single_block", C.c_int)]
 
 
 def _register():
@@ -49,7 +50,7 @@ def _register():
 class Plan:
     def __init__(self, pot, structs, precision: int = HDNNP_PREC_FP64, margin: float = 0.25, skin: float = 0.0,
                  masses=None, momenta=None, dt: float = 0.0, steps_per_launch: int = 1, want_dEdLat: bool = True,
-                 profile: bool = False, autotune: bool = False):
+                 profile: bool = False, autotune: bool = False, single_block: bool = True):
         import torch
 
         L = _register()
@@ -75,7 +76,8 @@ class Plan:
             self.hist = torch.zeros(steps_per_launch, self.nstruct, dtype=torch.float64, device=dev)
         ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
         self._opts = _Opts(int(precision), float(margin), float(skin), ptr(self.mom), ptr(self.mass), float(dt),
-                           int(steps_per_launch), ptr(self.hist), 1 if profile else 0, 1 if autotune else 0)
+                           int(steps_per_launch), ptr(self.hist), 1 if profile else 0, 1 if autotune else 0,
+                           0 if single_block else -1)
         self._per, self._lat = per, lat
         h = C.c_void_p()
         _check(L.hdnnp_plan_create(pot._m, C.byref(self._opts), self.nstruct, off.ctypes.data_as(C.c_void_p),

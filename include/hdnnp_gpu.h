@@ -224,6 +224,9 @@ typedef struct {
                                 batch for each candidate launch shape (neighbour-count split
                                 of the two launches, persistent grid per SM) and keep the
                                 fastest (hdnnp_plan_tuning)                               */
+    int single_block;        /* 0: an MD plan of one molecule of at most 64 atoms in FP64
+                                runs all steps of a launch in one thread block (one kernel
+                                launch, neighbour lists by direct search); -1: never  */
 } hdnnp_plan_opts;
 
 int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* opts, int nstruct, const int64_t* atom_off,
@@ -240,6 +243,8 @@ int hdnnp_plan_info(const hdnnp_plan* p, int64_t* entry_capacity, int* kernels_p
  * last evaluation of the last launch before each sync); the work counters
  * cover every evaluation.                                                     */
 int hdnnp_plan_profile(hdnnp_plan* p, double* stage_ms, int64_t* counters, int reset);
+/* Kernel launches per hdnnp_plan_launch are reported by hdnnp_plan_info
+ * (1 for the single-block MD of a small molecule).                           */
 /* Launch shape the autotuner chose (0, 0 without autotune: defaults) and the
  * symmetry-function time it measured for it (ms per evaluation).           */
 int hdnnp_plan_tuning(const hdnnp_plan* p, int* sf_split, int* sf_blocks_per_sm, double* sf_ms);

@@ -103,6 +103,41 @@ def test_md_plan_matches_host_verlet(pkg, PL, c1):
     pot.close()
 
 
+def test_single_block_md_matches_graph(pkg, PL, c1, pot, W):
+    """MD of a small molecule in one kernel per launch follows the graph of
+    separate kernels (same routines; direct-search lists sum neighbours in
+    another order, so to rounding) -- for the 8-atom example and a 60-atom
+    cluster of the ABX3 potential."""
+    from hdnnp_b200 import engine
+
+    s, m, p0 = c1
+    ex = engine.Hdnnp.from_runner(EXAMPLE_DIR)
+    blob = W.supercell(W.abx3_cell(), (1, 1, 5))  # 60 atoms
+    rng = np.random.default_rng(21)
+    mol = {"Z": blob["Z"], "pos": blob["pos"] + rng.normal(0.0, 0.05, blob["pos"].shape), "lat": None}
+    mm, pm = W.maxwell_boltzmann(mol["Z"], 300.0, 22)
+    for model, st, masses, mom, dt in ((ex, {"Z": s["Z"], "pos": s["pos"], "lat": None}, m, p0, 20.0),
+                                       (pot, mol, mm, pm, 0.5)):
+        kw = dict(masses=masses, momenta=mom, dt=dt, steps_per_launch=7, want_dEdLat=False)
+        with PL.Plan(model, [st], **kw) as a, PL.Plan(model, [st], single_block=False, **kw) as b:
+            assert a.info()["kernels_per_launch"] == 1 and b.info()["kernels_per_launch"] > 10
+            for _ in range(3):
+                a.launch()
+                b.launch()
+                assert a.sync() == 7 and b.sync() == 7
+                ea, eb = a.hist.cpu().numpy(), b.hist.cpu().numpy()
+                assert np.allclose(ea, eb, rtol=1e-9, atol=0)
+            assert np.abs(a.F.cpu().numpy() - b.F.cpu().numpy()).max() <= 1e-8
+            assert np.abs(a.pos.cpu().numpy() - b.pos.cpu().numpy()).max() <= 1e-9
+            assert np.abs(a.mom.cpu().numpy() - b.mom.cpu().numpy()).max() <= 1e-9 * max(1.0, np.abs(mom).max())
+            # a non-finite momentum is flagged like the graph path's check
+            a.mom[0, 0] = float("nan")
+            a.launch()
+            with pytest.raises(engine.HdnnpError):
+                a.sync()
+    ex.close()
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_skin_lists_match_rebuilt_lists(pot, PL, W, precision):
     s = cells(W, [(2, 2, 2)], 8)[0]
