@@ -220,11 +220,9 @@ struct SmallMdArgs {
     double* mom;
     const double* mass;
     double* force;
-    double* fprev;
     double* energy;
     double* hist;       // [nsteps] energies or null
     int* acc;           // [2]: OR of status flags, evaluations
-    int el_start[kMaxEl + 1];  // atoms grouped by element in Batch::el_atoms
 };
 
 // packed image shift: three signed 8-bit lattice multiples
@@ -267,7 +265,7 @@ int launch_committee_finish(const Batch& b, const Committee& cm, const double* E
 size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
-size_t small_md_smem_bytes(const DevModel& m, int mm);
+size_t small_md_smem_bytes(const DevModel& m, int natoms);  // dynamic shared memory of the kernel
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& a, cudaStream_t s);
 
 // Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).

@@ -185,30 +185,27 @@ int plan_autotune(hdnnp_plan* p) {
     return HDNNP_OK;
 }
 
-// Scratch and arguments of the single-block MD kernel: neighbour lists of up
-// to N*N entries, per-atom SF and network arrays, element groups (host-built
-// from Z; the kernel does not regroup).
+// Scratch and arguments of the single-block MD kernel (fused_md.cu): element
+// indices (host-built from Z) and the structure record it copies into shared
+// memory, and global homes of up to N*N neighbour entries and the per-atom SF
+// arrays for what its shared-memory layout cannot hold.
 int plan_setup_small(hdnnp_plan* p) {
     const DevModel& D = model_devmodel(p->model);
     const int N = p->natoms;
     std::vector<int32_t> Z((size_t)N);
     if (cudaMemcpy(Z.data(), p->Z, sizeof(int32_t) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
         return set_error(HDNNP_E_CUDA, "reading Z failed");
-    std::vector<int> elem((size_t)N), grouped;
+    std::vector<int> elem((size_t)N);
     for (int i = 0; i < N; ++i) {
         elem[i] = (Z[i] >= 1 && Z[i] <= 118) ? D.z2e[Z[i]] : -1;
         if (elem[i] < 0) return set_error(HDNNP_E_INPUT, "atom with an element that is not in the potential");
     }
-    for (int e = 0; e < D.nel; ++e) {
-        p->sa.el_start[e] = (int)grouped.size();
-        for (int i = 0; i < N; ++i)
-            if (elem[i] == e) grouped.push_back(i);
-    }
-    p->sa.el_start[D.nel] = (int)grouped.size();
-    // layout: doubles first, then StructInfo, then ints
+    // global scratch: the source copies of the element indices and the
+    // structure record, and the per-step arrays that the kernel's shared
+    // memory layout leaves in global memory (large molecules / wide SF sets)
     const size_t NN = (size_t)N * N, nsf = (size_t)D.nsf_max;
-    const size_t nd = 2 * N * nsf + N + 3 * NN + 3 * N + 9 * N;
-    const size_t ni = (N + 1) + 3 * NN + 3 * N + 4;
+    const size_t nd = 2 * N * nsf + 3 * NN + 9 * N;
+    const size_t ni = 3 * NN + N;
     const size_t bytes = nd * 8 + sizeof(StructInfo) + ni * 4;
     if (cudaMalloc(&p->sscratch, bytes) != cudaSuccess) return set_error(HDNNP_E_CUDA, "small-MD scratch allocation");
     double* d = (double*)p->sscratch;
@@ -220,36 +217,22 @@ int plan_setup_small(hdnnp_plan* p) {
     b.natoms = N;
     b.G = d; d += N * nsf;
     b.dEdG = d; d += N * nsf;
-    b.atE = d; d += N;
     b.gent = d; d += 3 * NN;
-    b.gself = d; d += 3 * N;
     b.vir = d;
     b.info = info;
-    b.nei_off = q; q += N + 1;
     b.nei_j = q; q += NN;
     b.nei_s = q; q += NN;
     b.nei_rev = q; q += NN;
-    b.elem = q; q += N;
-    b.sid = q; q += N;
-    b.el_atoms = q; q += N;
-    b.status = q;
+    b.elem = q;
     b.Z = p->Z;
-    b.pos = p->pos;
-    b.wpos = p->pos;  // molecule: no wrap; relative vectors are differences of positions
-    b.force = p->F;
-    b.energy = p->E;
     b.mmax = N - 1;
     b.nentries = (int)NN;
     StructInfo S{};
     for (int k = 0; k < 9; ++k) S.h[k] = S.hinv[k] = (k % 4 == 0) ? 1.0 : 0.0;
     S.ngrid[0] = S.ngrid[1] = S.ngrid[2] = 1;
     S.nat = N;
-    std::vector<int> zeros((size_t)N, 0);
     if (cudaMemcpy(info, &S, sizeof S, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b.elem, elem.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b.sid, zeros.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(b.el_atoms, grouped.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(b.status, 0, 4 * sizeof(int)) != cudaSuccess)
+        cudaMemcpy(b.elem, elem.data(), sizeof(int) * N, cudaMemcpyHostToDevice) != cudaSuccess)
         return set_error(HDNNP_E_CUDA, "small-MD set-up copies failed");
     SmallMdArgs& a = p->sa;
     a.natoms = N;
@@ -259,7 +242,6 @@ int plan_setup_small(hdnnp_plan* p) {
     a.mom = p->o.momenta_dev;
     a.mass = p->o.masses_dev;
     a.force = p->F;
-    a.fprev = p->fprev;
     a.energy = p->E;
     a.hist = p->o.energy_hist_dev;
     a.acc = p->acc;
@@ -360,10 +342,9 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
     // one small molecule in FP64: every MD step of a launch in one kernel
     {
         const DevModel& D = model_devmodel(m);
-        const int mm = ((p->natoms - 1 + 31) / 32) * 32 < 32 ? 32 : ((p->natoms - 1 + 31) / 32) * 32;
         p->small = o->momenta_dev && nstruct == 1 && !periodic[0] && p->natoms <= kSmallMolecule &&
                    o->precision == HDNNP_PREC_FP64 && !o->profile && o->single_block >= 0 &&
-                   small_md_smem_bytes(D, mm) <= 200 * 1024;
+                   small_md_smem_bytes(D, p->natoms) <= 226 * 1024;
         if (p->small) {
             if ((r = plan_setup_small(p))) return bail(r, hdnnp_last_error());
             p->kernels_per_launch = 1;
