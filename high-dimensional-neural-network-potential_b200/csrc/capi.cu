@@ -127,6 +127,11 @@ int struct_setup(int nat, const double* pos, int periodic, const double* lat, do
     for (int d = 0; d < 3; ++d)
         for (int r = 0; r < 3; ++r) grid[r + 3 * d] = S.h[r + 3 * d] / S.ngrid[d];
     n_cells(grid, rc, S.nsearch);
+    // A molecule's cells beyond its grid are empty: offsets of ngrid or more
+    // find nothing (the reference visits and skips them), so the search stops
+    // there -- flat or linear molecules (an extent of 2e-4 Bohr) stay cheap.
+    if (!periodic)
+        for (int d = 0; d < 3; ++d) S.nsearch[d] = std::min(S.nsearch[d], S.ngrid[d] - 1);
     if (periodic) {
         int nl[3];
         n_cells(S.h, rc, nl);

@@ -465,6 +465,8 @@ __global__ void k_molecule_boxes(Batch b, double rc) {
     for (int d = 0; d < 3; ++d)
         for (int r = 0; r < 3; ++r) grid[r + 3 * d] = dv(S.h[r + 3 * d], (double)S.ngrid[d]);
     d_n_cells(grid, rc, S.nsearch);
+    // cells beyond the molecule's grid are empty (see the host set-up)
+    for (int d = 0; d < 3; ++d) S.nsearch[d] = min(S.nsearch[d], S.ngrid[d] - 1);
     for (int d = 0; d < 3; ++d)
         if (S.nsearch[d] > 64) {
             atomicOr(&b.status[0], 32);  // reported as a capacity error

@@ -60,6 +60,28 @@ def test_example_molecule(eng, gex, ex_model, c1):
     assert np.abs(F - np.array(fx["forces"])).max() <= F_ABS
 
 
+def test_flat_and_linear_molecules(eng, gex, ex_model, c1, pkg):
+    """A planar molecule (z extent 0) and a 2-atom one (extent 0 in two
+    directions): the artificial box is 2e-4 Bohr thick there, so the cell
+    search would span ~10^5 cells; the engine stops at the grid (same list)."""
+    from hdnnp_b200 import plan as PL
+
+    s = c1[0]
+    flat = s["pos"].copy()
+    flat[:, 2] = 0.25
+    two = np.array([[0.0, 0.0, 0.0], [2.7, 0.0, 0.0]])
+    # the oracle searches every cell like the reference, which for the
+    # linear molecule means ~10^10 empty cells: it gets a rotated copy
+    R, _ = np.linalg.qr(np.random.default_rng(5).normal(size=(3, 3)))
+    for Z, pos, rot in ((s["Z"], flat, np.eye(3)), (s["Z"][:2], two, R)):
+        E, F, _ = gex.energy_and_forces(eng.AtStruct(Z, pos))
+        ref = ex_model.eval(Z, pos @ rot.T)
+        check(E, F, None, {"energy": ref["energy"], "forces": ref["forces"] @ rot})
+        with PL.Plan(gex, [{"Z": Z, "pos": pos, "lat": None}]) as p:  # device-built box
+            Ep, Fp, _ = p.results()
+        assert Ep[0] == E and np.array_equal(Fp, F)
+
+
 def test_small_cell_images_and_stress(eng, gab, abx3_model, W, orc):
     c = small_cell(W)
     E, F, dl = gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], c["lat"]), dEdLat=True)

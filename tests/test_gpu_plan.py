@@ -105,9 +105,10 @@ def test_md_plan_matches_host_verlet(pkg, PL, c1):
 
 def test_single_block_md_matches_graph(pkg, PL, c1, pot, W):
     """MD of a small molecule in one kernel per launch follows the graph of
-    separate kernels (same routines; direct-search lists sum neighbours in
-    another order, so to rounding) -- for the 8-atom example and a 60-atom
-    cluster of the ABX3 potential."""
+    separate kernels (same formulas; other summation orders, so to rounding):
+    the item-parallel form for the 8-atom example, a 2-atom fragment of it (no
+    angular pairs) and an 8-atom fragment of the ABX3 cell (280 functions per
+    element); the warp-per-atom form for a 60-atom ABX3 cluster."""
     from hdnnp_b200 import engine
 
     s, m, p0 = c1
@@ -116,8 +117,13 @@ def test_single_block_md_matches_graph(pkg, PL, c1, pot, W):
     rng = np.random.default_rng(21)
     mol = {"Z": blob["Z"], "pos": blob["pos"] + rng.normal(0.0, 0.05, blob["pos"].shape), "lat": None}
     mm, pm = W.maxwell_boltzmann(mol["Z"], 300.0, 22)
-    for model, st, masses, mom, dt in ((ex, {"Z": s["Z"], "pos": s["pos"], "lat": None}, m, p0, 20.0),
-                                       (pot, mol, mm, pm, 0.5)):
+    frag = {"Z": mol["Z"][:8], "pos": mol["pos"][:8], "lat": None}
+    two = {"Z": s["Z"][:2], "pos": s["pos"][:2], "lat": None}
+    cases = ((ex, {"Z": s["Z"], "pos": s["pos"], "lat": None}, m, p0, 20.0),
+             (ex, two, m[:2], p0[:2], 20.0),
+             (pot, frag, mm[:8], pm[:8], 0.5),
+             (pot, mol, mm, pm, 0.5))
+    for model, st, masses, mom, dt in cases:
         kw = dict(masses=masses, momenta=mom, dt=dt, steps_per_launch=7, want_dEdLat=False)
         with PL.Plan(model, [st], **kw) as a, PL.Plan(model, [st], single_block=False, **kw) as b:
             assert a.info()["kernels_per_launch"] == 1 and b.info()["kernels_per_launch"] > 10
