@@ -77,29 +77,61 @@ def workload(W, n, seed):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML every 20 ms (reads only), or nvidia-smi every 200 ms where
+    the NVML bindings are missing."""
+
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.idx = gpu_index
-        self.samples = []
+        # the CUDA device index names a physical GPU through CUDA_VISIBLE_DEVICES
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+        self.idx = int(vis[gpu_index]) if gpu_index < len(vis) and vis[gpu_index].strip().isdigit() else gpu_index
+        self.samples = []  # (sm MHz, max sm MHz, set of reason names)
+        self.source = None
         self._stop = threading.Event()
         self._th = None
 
-    def start(self):
-        q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
-            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-            "clocks_event_reasons.sw_power_cap"
+    def _nvml_loop(self):
+        import pynvml as N
 
-        def run():
+        N.nvmlInit()
+        try:
+            h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            bits = (N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap)
+            self.source = "nvml, every 20 ms"
             while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                    if out.returncode == 0 and out.stdout.strip():
-                        self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+                sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, mx, {n for n, b in zip(self.NAMES, bits) if r & b}))
+                self._stop.wait(0.02)
+        finally:
+            N.nvmlShutdown()
+
+    def _smi_loop(self):
+        q = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        self.source = "nvidia-smi, every 200 ms"
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                if out.returncode == 0 and len(f) >= 6:
+                    self.samples.append((float(f[0]), float(f[1]),
+                                         {n for n, v in zip(self.NAMES, f[2:6]) if v == "Active"}))
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def start(self):
+        def run():
+            try:
+                self._nvml_loop()
+            except Exception:
+                self._smi_loop()
 
         self._th = threading.Thread(target=run, daemon=True)
         self._th.start()
@@ -110,12 +142,10 @@ class ClockSampler:
             self._th.join(timeout=10)
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 5 + k and s[5 + k] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        sm = [x[0] for x in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(x[1] for x in self.samples),
+                "reasons": sorted(set().union(*[x[2] for x in self.samples])), "samples": len(self.samples),
+                "source": self.source}
 
 
 def measured_peaks(torch):
