@@ -442,8 +442,8 @@ int upload_model(hdnnp_model* m) {
         ok = ok && (kH + np) <= 512 && kp <= 512;
         const size_t szA = (size_t)2 * 128 * kp * 2, szBf = (size_t)2 * kH * kp * 2, szBb = (size_t)2 * np * kH * 2,
                      szAb = (size_t)2 * 128 * kH * 2;
-        size_t wsmall = D.width[1];
-        for (int l = 1; l < L; ++l) wsmall += (size_t)D.width[l + 1] * D.width[l] + D.width[l + 1];
+        // b1, then each later layer's W and bias zero-padded to kH x kH and kH
+        const size_t wsmall = kH + (size_t)(L - 1) * (kH * kH + kH);
         const size_t total = std::max(szA, szBb + szAb) + szBf + ((wsmall * 4 + 15) & ~size_t(15)) + 64;
         ok = ok && total <= 227 * 1024;
         if (ok) {

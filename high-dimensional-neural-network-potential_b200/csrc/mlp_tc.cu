@@ -132,7 +132,8 @@ __device__ __forceinline__ float act_dv(char a, float c, float y) {
 // Shared-memory plan (bytes):
 //   [0, szA)            A_fwd hi | lo  (128 x Kp each); reused for B_bwd hi|lo and A_bwd hi|lo
 //   [szA, szA+szBf)     B_fwd hi | lo  (32 x Kp each)
-//   then FP32 small weights of layers 2..L, then the mbarrier and the TMEM slot
+//   then FP32 small weights of layers 2..L (b1 and each layer's W [32][32]
+//   and bias [32], zero-padded: rows read as float4), the mbarrier, the TMEM slot
 struct TCPlan {
     int Kp, Np, nch, chN;
     size_t szA, szBf, szBb, szAb, szW, total;
@@ -148,9 +149,7 @@ __host__ __device__ inline TCPlan tc_plan(const DevModel& m) {
     p.szBf = (size_t)2 * kH * p.Kp * 2;
     p.szBb = (size_t)2 * p.Np * kH * 2;
     p.szAb = (size_t)2 * kM * kH * 2;
-    size_t w = 0;
-    for (int l = 1; l < m.nlayers; ++l) w += (size_t)m.width[l + 1] * m.width[l] + m.width[l + 1];
-    w += m.width[1];  // b1
+    const size_t w = kH + (size_t)(m.nlayers - 1) * (kH * kH + kH);  // b1, then W_l and b_l padded
     p.szW = ((w * 4) + 15) & ~size_t(15);
     size_t reuse = p.szBb + p.szAb;
     p.total = (p.szA > reuse ? p.szA : reuse) + p.szBf + p.szW + 64;
@@ -204,16 +203,19 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
         for (int i = tid; i < (int)(P.szBf / 16); i += kThr) dst[i] = src[i];
         int o = 0;
         const float* b1 = m.bf + m.b_off[e * L + 0];
-        for (int i = tid; i < H; i += kThr) sW[i] = b1[i];
-        o += H;
+        for (int i = tid; i < kH; i += kThr) sW[i] = i < H ? b1[i] : 0.f;
+        o += kH;
         for (int l = 1; l < L; ++l) {
             const int wi = m.width[l], wo = m.width[l + 1];
             const float* W = m.wf + m.w_off[e * L + l];
             const float* bb = m.bf + m.b_off[e * L + l];
-            for (int i = tid; i < wi * wo; i += kThr) sW[o + i] = W[i];
-            o += wi * wo;
-            for (int i = tid; i < wo; i += kThr) sW[o + i] = bb[i];
-            o += wo;
+            for (int i = tid; i < kH * kH; i += kThr) {
+                const int r = i / kH, q = i % kH;
+                sW[o + i] = (r < wo && q < wi) ? W[r * wi + q] : 0.f;
+            }
+            o += kH * kH;
+            for (int i = tid; i < kH; i += kThr) sW[o + i] = i < wo ? bb[i] : 0.f;
+            o += kH;
         }
     }
     // ---- stage A_fwd: thread = row; its row of G' (FP32) -> FP16 hi | lo in
@@ -291,18 +293,10 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
     const bool live = row < cnt;
     const int atom = live ? b.el_atoms[t0 + row] : 0;
     if (ok) {
-        // offsets of the FP32 weights of layers 1..L-1 in sW
-        int woff[NL], boff[NL];
-        {
-            int o = H;
-#pragma unroll
-            for (int l = 1; l < NL; ++l) {
-                woff[l] = o;
-                o += m.width[l] * m.width[l + 1];
-                boff[l] = o;
-                o += m.width[l + 1];
-            }
-        }
+        // offsets of the padded FP32 weights of layers 1..L-1 in sW
+        constexpr int kWB = kH * kH + kH;
+        auto woff = [](int l) { return kH + (l - 1) * kWB; };
+        auto boff = [](int l) { return kH + (l - 1) * kWB + kH * kH; };
         float v[32];
         tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), v);
         const float inv = m.tc_inv_s1[e];
@@ -315,25 +309,35 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
             yp[o] = yv;
             dact[0][o] = o < H ? act_dv(m.act[0], c, yv) : 0.f;
         }
+        // Layers 2..L: the padded rows are read as float4 (broadcast: every
+        // thread reads the same weights); neurons beyond the layer's width
+        // are skipped by a branch uniform over the CTA.  Padding adds only
+        // zero terms, in the same order as the unpadded sums.
 #pragma unroll
         for (int l = 1; l < NL; ++l) {
-            const int wi = m.width[l], wo = m.width[l + 1];
-            const float* W = sW + woff[l];
-            const float* bb = sW + boff[l];
+            const int wo = m.width[l + 1];
+            const float4* W4 = (const float4*)(sW + woff(l));
+            const float* bb = sW + boff(l);
             const char al = m.act[l];
             float yc[kH];
 #pragma unroll
             for (int o = 0; o < kH; ++o) {
-                float c = 0.f;
+                float c = 0.f, yv = 0.f, dv = 0.f;
                 if (o < wo) {
                     c = bb[o];
 #pragma unroll
-                    for (int i = 0; i < kH; ++i)
-                        if (i < wi) c += W[o * wi + i] * yp[i];
+                    for (int q = 0; q < kH / 4; ++q) {
+                        const float4 w = W4[o * (kH / 4) + q];
+                        c += w.x * yp[4 * q];
+                        c += w.y * yp[4 * q + 1];
+                        c += w.z * yp[4 * q + 2];
+                        c += w.w * yp[4 * q + 3];
+                    }
+                    yv = act_fw(al, c);
+                    dv = act_dv(al, c, yv);
                 }
-                const float yv = o < wo ? act_fw(al, c) : 0.f;
                 yc[o] = yv;
-                dact[l][o] = o < wo ? act_dv(al, c, yv) : 0.f;
+                dact[l][o] = dv;
             }
 #pragma unroll
             for (int o = 0; o < kH; ++o) yp[o] = yc[o];
@@ -345,21 +349,27 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
         for (int o = 0; o < kH; ++o) d[o] = dact[NL - 1][o];
 #pragma unroll
         for (int l = NL - 1; l >= 1; --l) {
-            const int wi = m.width[l], wo = m.width[l + 1];
-            const float* W = sW + woff[l];
+            const int wo = m.width[l + 1];
+            const float4* W4 = (const float4*)(sW + woff(l));
             float g[kH];
 #pragma unroll
-            for (int i = 0; i < kH; ++i) {
-                float sacc = 0.f;
-                if (i < wi) {
+            for (int i = 0; i < kH; ++i) g[i] = 0.f;
+            // g_i = sum over o (ascending) of W[o][i] d_o, four i per float4 row load
 #pragma unroll
-                    for (int o = 0; o < kH; ++o)
-                        if (o < wo) sacc += W[o * wi + i] * d[o];
+            for (int o = 0; o < kH; ++o) {
+                if (o < wo) {
+#pragma unroll
+                    for (int q = 0; q < kH / 4; ++q) {
+                        const float4 w = W4[o * (kH / 4) + q];
+                        g[4 * q] += w.x * d[o];
+                        g[4 * q + 1] += w.y * d[o];
+                        g[4 * q + 2] += w.z * d[o];
+                        g[4 * q + 3] += w.w * d[o];
+                    }
                 }
-                g[i] = sacc * dact[l - 1][i];
             }
 #pragma unroll
-            for (int i = 0; i < kH; ++i) d[i] = g[i];
+            for (int i = 0; i < kH; ++i) d[i] = g[i] * dact[l - 1][i];
         }
         // ---- stage A_bwd (delta1 scaled, hi | lo) and B_bwd in the A_fwd region
         __half* Bhi = (__half*)sA;
