@@ -184,6 +184,7 @@ struct hdnnp_ctx {
     int mlp_simt = 0;
     int sf_split = 0;          // launch shape of the fast SF kernels (0: defaults)
     int sf_blocks_per_sm = 0;
+    int nei_warp = 0;          // neighbour-list form (0: by batch size)
     int launches = 0;
     // device buffers
     DevBuf<StructInfo> info;
@@ -606,6 +607,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.dEdLat = dEdLat_d;
     b.sf_split = c->sf_split;
     b.sf_blocks_per_sm = c->sf_blocks_per_sm;
+    b.nei_warp = c->nei_warp;
     b.rc_list = pp ? pp->rc_list : 0.0;
     b.rebuild = pp ? pp->rebuild : nullptr;
     b.wshift = pp ? pp->wshift : nullptr;
@@ -862,6 +864,11 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
     if (std::string(name) == "sf_blocks_per_sm") {
         if (value < 0 || value > 64) return fail(HDNNP_E_INPUT, "sf_blocks_per_sm must be 0..64");
         c->sf_blocks_per_sm = value;
+        return HDNNP_OK;
+    }
+    if (std::string(name) == "nei_warp") {
+        if (value < -1 || value > 1) return fail(HDNNP_E_INPUT, "nei_warp must be -1, 0 or 1");
+        c->nei_warp = value;
         return HDNNP_OK;
     }
     return fail(HDNNP_E_INPUT, std::string("unknown option ") + name);

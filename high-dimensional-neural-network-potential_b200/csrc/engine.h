@@ -178,6 +178,7 @@ struct Batch {
     // persistent grid in blocks per SM.  Set by the plans' autotuner.
     int sf_split;
     int sf_blocks_per_sm;
+    int nei_warp;             // neighbour lists: 1 warp per atom, -1 thread per atom, 0 by batch size
 };
 
 constexpr int kPairCap = 1024;  // listed pairs per atom (the dense workloads average ~550)

@@ -104,21 +104,46 @@ __global__ void k_fill_cells(Batch b, int* cursor) {
     b.cell_atoms[b.cell_start[c] + p] = i;
 }
 
-// deterministic order inside a cell: increasing atom index
+// Deterministic order inside a cell: increasing atom index.  One warp per
+// cell: the cell's atoms are copied to shared memory and each goes to its
+// rank (the number of smaller indices; indices are distinct).  Cells above
+// kSortCap atoms are sorted by one lane in place (insertion sort).
+constexpr int kSortCap = 256;
+constexpr int kSortWarps = kThreads / 32;
 __global__ void k_sort_cells(Batch b) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= b.ncells || keep_list(b)) return;
-    int s = b.cell_start[c], e = b.cell_start[c + 1];
-    for (int p = s + 1; p < e; ++p) {
-        int v = b.cell_atoms[p];
-        int q = p - 1;
-        while (q >= s && b.cell_atoms[q] > v) {
-            b.cell_atoms[q + 1] = b.cell_atoms[q];
-            --q;
-        }
-        b.cell_atoms[q + 1] = v;
+    __shared__ int buf[kSortWarps][kSortCap];
+    const int c = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (c >= b.ncells || keep_list(b)) return;  // uniform per warp
+    const int s = b.cell_start[c], e = b.cell_start[c + 1], n = e - s;
+    if (n <= 1) return;
+    if (n > kSortCap) {
+        if (lane == 0)
+            for (int p = s + 1; p < e; ++p) {
+                const int v = b.cell_atoms[p];
+                int q = p - 1;
+                while (q >= s && b.cell_atoms[q] > v) {
+                    b.cell_atoms[q + 1] = b.cell_atoms[q];
+                    --q;
+                }
+                b.cell_atoms[q + 1] = v;
+            }
+        return;
+    }
+    int* t = buf[w];
+    for (int p = lane; p < n; p += 32) t[p] = b.cell_atoms[s + p];
+    __syncwarp();
+    for (int p = lane; p < n; p += 32) {
+        const int v = t[p];
+        int r = 0;
+        for (int q = 0; q < n; ++q) r += t[q] < v;
+        b.cell_atoms[s + r] = v;
     }
 }
+
+// floor(a / n) for n > 0, in integers (the same value as the floating-point
+// floor of the exact quotient)
+__device__ __forceinline__ int floor_div(int a, int n) { return a >= 0 ? a / n : -((n - 1 - a) / n); }
 
 // K3 enumeration shared by the count and the fill pass.
 template <bool kFill>
@@ -143,17 +168,17 @@ __global__ void k_neighbours(Batch b, DevModel m) {
                 int dx = 0, dy = 0, dz = 0;
                 if (cz < 0 || cz >= S.ngrid[2]) {
                     if (!S.periodic) continue;
-                    dz = (int)floor((double)cz / S.ngrid[2]);
+                    dz = floor_div(cz, S.ngrid[2]);
                     cz -= S.ngrid[2] * dz;
                 }
                 if (cy < 0 || cy >= S.ngrid[1]) {
                     if (!S.periodic) continue;
-                    dy = (int)floor((double)cy / S.ngrid[1]);
+                    dy = floor_div(cy, S.ngrid[1]);
                     cy -= S.ngrid[1] * dy;
                 }
                 if (cx < 0 || cx >= S.ngrid[0]) {
                     if (!S.periodic) continue;
-                    dx = (int)floor((double)cx / S.ngrid[0]);
+                    dx = floor_div(cx, S.ngrid[0]);
                     cx -= S.ngrid[0] * dx;
                 }
                 // image shift, summed z, y, x like the reference
@@ -183,6 +208,113 @@ __global__ void k_neighbours(Batch b, DevModel m) {
         }
     }
     if (!kFill) b.nei_cnt[i] = n;
+}
+
+// The same enumeration with one warp per atom: the virtual cells, in the
+// reference's order (jx outer, jz inner), are dealt to the lanes 32 at a time;
+// each lane walks its cell's atoms in cell order, and the fill pass places a
+// round's accepted atoms by an ordered prefix sum over the lanes -- so the
+// list is the same, entry for entry.  For batches too small to fill the GPU
+// with a thread per atom (a single cell of a few hundred atoms has thousands
+// of candidates per atom, walked serially by one thread).
+template <bool kFill>
+__global__ void k_neighbours_warp(Batch b, DevModel m) {
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= b.natoms || keep_list(b)) return;  // uniform per warp
+    if (kFill && b.status[3]) return;
+    const StructInfo& S = b.info[b.sid[i]];
+    const double rc = b.rc_list > 0.0 ? b.rc_list : m.max_rc, rc2 = rc * rc;
+    const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
+    const int c = b.cell_of[i] - S.cell_off;
+    const int ix = c / (S.ngrid[1] * S.ngrid[2]);
+    const int iy = (c / S.ngrid[2]) % S.ngrid[1];
+    const int iz = c % S.ngrid[2];
+    const double* h = S.h;
+    const int ny = 2 * S.nsearch[1] + 1, nz = 2 * S.nsearch[2] + 1;
+    const int nv = (2 * S.nsearch[0] + 1) * ny * nz;
+    int n = 0;
+    int out = kFill ? b.nei_off[i] : 0;
+    for (int v0 = 0; v0 < nv; v0 += 32) {
+        const int v = v0 + lane;
+        int p0 = 0, p1 = 0, dx = 0, dy = 0, dz = 0;
+        double lx = 0, ly = 0, lz = 0;
+        bool home = false;
+        if (v < nv) {
+            const int jx = v / (ny * nz) - S.nsearch[0];
+            const int jy = (v / nz) % ny - S.nsearch[1];
+            const int jz = v % nz - S.nsearch[2];
+            int cx = ix + jx, cy = iy + jy, cz = iz + jz;
+            bool inside = true;
+            if (cz < 0 || cz >= S.ngrid[2]) {
+                inside = S.periodic;
+                dz = floor_div(cz, S.ngrid[2]);
+                cz -= S.ngrid[2] * dz;
+            }
+            if (cy < 0 || cy >= S.ngrid[1]) {
+                inside = inside && S.periodic;
+                dy = floor_div(cy, S.ngrid[1]);
+                cy -= S.ngrid[1] * dy;
+            }
+            if (cx < 0 || cx >= S.ngrid[0]) {
+                inside = inside && S.periodic;
+                dx = floor_div(cx, S.ngrid[0]);
+                cx -= S.ngrid[0] * dx;
+            }
+            if (inside) {
+                if (dz) { lx += h[6] * dz; ly += h[7] * dz; lz += h[8] * dz; }
+                if (dy) { lx += h[3] * dy; ly += h[4] * dy; lz += h[5] * dy; }
+                if (dx) { lx += h[0] * dx; ly += h[1] * dx; lz += h[2] * dx; }
+                home = (jx == 0 && jy == 0 && jz == 0);
+                const int cell = S.cell_off + (cx * S.ngrid[1] + cy) * S.ngrid[2] + cz;
+                p0 = b.cell_start[cell];
+                p1 = b.cell_start[cell + 1];
+            }
+        }
+        // this lane's accepted atoms of its virtual cell
+        int cnt = 0;
+        for (int p = p0; p < p1; ++p) {
+            const int j = b.cell_atoms[p];
+            if (j == i && home) continue;
+            double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
+            double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
+            cnt += ddx * ddx + ddy * ddy + ddz * ddz < rc2;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (kFill && cnt > 0) {
+            int o = out + incl - cnt;
+            const int sh = pack_shift(dx, dy, dz);
+            for (int p = p0; p < p1; ++p) {
+                const int j = b.cell_atoms[p];
+                if (j == i && home) continue;
+                double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
+                double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
+                if (ddx * ddx + ddy * ddy + ddz * ddz < rc2) {
+                    b.nei_j[o] = j;
+                    b.nei_s[o] = sh;
+                    ++o;
+                }
+            }
+        }
+        out += total;
+        n += total;
+    }
+    if (!kFill && lane == 0) b.nei_cnt[i] = n;
+}
+
+// Batches below this many atoms list neighbours with a warp per atom
+// (measured on B200, count + fill: the 768-atom cell 0.14 against 0.47 ms, the
+// 49,152-atom cell 0.60 against 0.73 ms; the 758,676-atom batch of 4096 cells
+// 7.4 against 6.2 ms, where threads already fill the GPU).
+constexpr int kWarpListAtoms = 131072;
+inline bool warp_lists(const Batch& b) {
+    return b.nei_warp > 0 || (b.nei_warp == 0 && b.natoms < kWarpListAtoms);
 }
 
 // Reverse-entry index: for entry e = (a -> j, shift s) the entry (j -> a, -s)
@@ -304,9 +436,12 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s) 
     cudaMemsetAsync(b.cell_cnt, 0, sizeof(int) * (b.ncells + 1), s);
     k_fill_cells<<<gA, kThreads, 0, s>>>(b, b.cell_cnt);
     ++L;
-    k_sort_cells<<<(b.ncells + kThreads - 1) / kThreads, kThreads, 0, s>>>(b);
+    k_sort_cells<<<(unsigned)((32LL * b.ncells + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     ++L;
-    k_neighbours<false><<<gA, kThreads, 0, s>>>(b, m);
+    if (warp_lists(b))
+        k_neighbours_warp<false><<<(unsigned)((32LL * b.natoms + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
+    else
+        k_neighbours<false><<<gA, kThreads, 0, s>>>(b, m);
     ++L;
     cudaMemcpyAsync(b.nei_off, b.nei_cnt, sizeof(int) * b.natoms, cudaMemcpyDeviceToDevice, s);
     L += launch_scan(b.nei_off, b.natoms, b.scan_tmp, nullptr, s);
@@ -319,8 +454,11 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s) 
 
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) {
     const int gA = (b.natoms + kThreads - 1) / kThreads;
-    k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
     const long long warps_threads = 32LL * b.natoms;
+    if (warp_lists(b))
+        k_neighbours_warp<true><<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
+    else
+        k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
     k_reverse<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     return 2;
 }

@@ -85,7 +85,9 @@ int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
  * the lambda x zeta x eta kernels; "runtime_zeta" = 1 makes the
  * lambda x zeta x eta kernels read the zeta set from the model even when a
  * kernel with that zeta set compiled in exists.  Results agree within
- * rounding.                                                                  */
+ * rounding.  "nei_warp" chooses how neighbour lists are built: 1 one warp per
+ * atom, -1 one thread per atom, 0 (default) a warp per atom below 131,072
+ * atoms in the batch; both give the same lists, entry for entry.             */
 int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
 
 /* ---------------------------------------------------------------- evaluation

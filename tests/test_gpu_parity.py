@@ -178,6 +178,24 @@ def test_generic_and_fast_kernels_agree(eng, gab, abx3_model, W):
     assert np.abs(fast["dEdLat"] - gen["dEdLat"]).max() <= L_ABS
 
 
+def test_neighbour_list_forms_agree(eng, gab, W):
+    """Neighbour lists built with a warp per atom and with a thread per atom
+    are the same entry for entry, so every output is bitwise equal (periodic
+    cells of several sizes and a molecule in one batch)."""
+    s = W.config_c4(n_struct=12, seed=17) + [W.config_c2()]
+    mol = W.abx3_cell()
+    s.append({"Z": mol["Z"], "pos": mol["pos"] + 2.0, "lat": None})
+    out = {}
+    try:
+        for v in (1, -1):
+            gab.set_option("nei_warp", v)
+            out[v] = gab.eval_batch(s, dEdLat=True)
+    finally:
+        gab.set_option("nei_warp", 0)
+    for k in ("energy", "forces", "dEdLat"):
+        assert np.array_equal(out[1][k], out[-1][k])
+
+
 def test_compiled_and_runtime_zeta_kernels_agree(eng, gab, W):
     s = W.config_c4(n_struct=6, seed=16)
     fixed = gab.eval_batch(s, dEdLat=True)
