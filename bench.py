@@ -186,6 +186,15 @@ FLOPS = {
 }
 
 
+# DRAM bytes (read + write) per atom of each symmetry-function stage in the
+# mixed form, from one ncu capture of both launches of each kernel on the
+# first 1024 structures of this workload (191,160 atoms; values 706.5 MB,
+# gradients 842.5 MB), scaled by the atoms of a step: the traffic of these
+# kernels is per atom (positions, neighbour entries, G / dE/dG rows, pair
+# lists), so it grows in proportion.
+TRAFFIC_PER_ATOM = {"sf_values": 706.5e6 / 191160, "sf_gradients": 842.5e6 / 191160}
+
+
 def kernel_flops(stage, counters, evals):
     per = FLOPS[stage]
     return sum(per[k] * counters[k] for k in per) / max(evals, 1)
@@ -595,10 +604,15 @@ def main():
     peaks = measured_peaks(torch) if rank == 0 else {}
     peak_key = "fp64" if args.precision == "fp64" else "fp32"
     achieved = flops / (dom_ms / 1e3) / 1e12
+    traffic = TRAFFIC_PER_ATOM[dom] * counters["atoms"] / evals if args.precision == "mixed" else None
     roof = {"bound": peak_key + "-alu", "kernel": dom, "achieved": achieved, "peak": peaks.get(peak_key),
             "unit": "TFLOP/s", "frac": achieved / peaks[peak_key] if peaks.get(peak_key) else None,
             "peak_source": f"measured in this run: cuBLAS {peak_key.upper()} GEMM (no TF32), best of 5",
-            "traffic": None, "flops_per_launch": flops, "ms_per_launch": dom_ms,
+            "traffic": traffic, "traffic_unit": "bytes per step, DRAM read + write",
+            "traffic_source": "ncu capture of the same kernel on 1024 of the structures, scaled by atoms"
+            if traffic else "not captured for this precision",
+            "dram_GBs": traffic / (dom_ms / 1e3) / 1e9 if traffic else None,
+            "flops_per_launch": flops, "ms_per_launch": dom_ms,
             "stage_ms_per_step": {k: v / evals for k, v in stage_ms.items()},
             "units_per_step": {k: v / evals for k, v in counters.items() if k != "evaluations"}}
 
