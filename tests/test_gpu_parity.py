@@ -82,6 +82,20 @@ def test_flat_and_linear_molecules(eng, gex, ex_model, c1, pkg):
         assert Ep[0] == E and np.array_equal(Fp, F)
 
 
+def test_crowded_cell_of_a_sparse_molecule(eng, gab, abx3_model):
+    """Two clusters 1000 Bohr apart: the molecule's box is so sparse that its
+    grid is coarsened to ~60-Bohr cells, and the 280-atom cluster (4 Bohr
+    spacing) lands in one cell -- above the 256 atoms the shared-memory cell
+    sort takes, so the in-place fallback orders it."""
+    rng = np.random.default_rng(23)
+    g = np.stack(np.meshgrid(*[np.arange(7)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    pos = np.concatenate([g[:280] * 4.0 + rng.normal(0.0, 0.1, (280, 3)),
+                          1000.0 + g[:20] * 4.0 + rng.normal(0.0, 0.1, (20, 3))])
+    Z = rng.choice([1, 6, 7, 53, 82], 300).astype(np.int32)
+    E, F, _ = gab.energy_and_forces(eng.AtStruct(Z, pos))
+    check(E, F, None, abx3_model.eval(Z, pos))
+
+
 def test_small_cell_images_and_stress(eng, gab, abx3_model, W, orc):
     c = small_cell(W)
     E, F, dl = gab.energy_and_forces(eng.AtStruct(c["Z"], c["pos"], c["lat"]), dEdLat=True)
