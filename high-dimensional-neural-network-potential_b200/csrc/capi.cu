@@ -1254,7 +1254,7 @@ int set_error(int code, const std::string& msg) { return fail(code, msg); }
 // read only for its bounding box (null for periodic structures).
 int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* Z_dev, const double* pos_dev,
                   const double* const* mol_pos, const int32_t* periodic, const double* lat, double* energy_dev,
-                  double* force_dev, double* dEdLat_dev, cudaStream_t st) {
+                  double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan* pp, double rc_list) {
     if (!c || nstruct <= 0 || !off || !Z_dev || !pos_dev || !periodic || !lat || !energy_dev || !force_dev)
         return fail(HDNNP_E_INPUT, "null argument or empty batch");
     CUDA_TRY(cudaSetDevice(c->model->device));
@@ -1265,12 +1265,33 @@ int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* 
         const int64_t a0 = off[s], a1 = off[s + 1];
         if (a1 <= a0) return fail(HDNNP_E_INPUT, "structure " + std::to_string(s) + " has no atoms");
         const double* mp = periodic[s] ? nullptr : (mol_pos ? mol_pos[s] : nullptr);
-        int r = struct_setup((int)(a1 - a0), mp, periodic[s], lat + 9 * s, H.max_rc, c->hinfo[s]);
+        int r = struct_setup((int)(a1 - a0), mp, periodic[s], lat + 9 * s, rc_list > 0.0 ? rc_list : H.max_rc,
+                             c->hinfo[s]);
         if (r) return fail(r, "structure " + std::to_string(s) + ": " + g_err);
         c->hinfo[s].atom_off = (int)a0;
         c->hinfo[s].nat = (int)(a1 - a0);
     }
-    return run_pipeline(c, nstruct, (int)off[nstruct], Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st);
+    return run_pipeline(c, nstruct, (int)off[nstruct], Z_dev, pos_dev, energy_dev, force_dev, dEdLat_dev, st, pp);
+}
+
+// Neighbour-list arrays of c (device), for callers that keep lists between
+// evaluations (the server's Verlet skin): after a build they hold the lists
+// of the last evaluation; before an evaluation in keep mode (PipePlan with a
+// rebuild flag of 0) the caller fills elem, nei_cnt, nei_j, nei_s and nei_rev
+// for natoms atoms and nentries entries (nei_off follows from nei_cnt).
+int ctx_list_arrays(hdnnp_ctx* c, size_t natoms, size_t nentries, CtxLists* out) {
+    int r;
+    if ((r = c->elem.ensure(natoms)) || (r = c->nei_cnt.ensure(natoms + 1)) || (r = c->nei_off.ensure(natoms + 1)) ||
+        (r = c->nei_j.ensure(nentries + 1)) || (r = c->nei_s.ensure(nentries + 1)) ||
+        (r = c->nei_rev.ensure(nentries + 1)))
+        return r;
+    out->elem = c->elem.p;
+    out->cnt = c->nei_cnt.p;
+    out->off = c->nei_off.p;
+    out->nj = c->nei_j.p;
+    out->ns = c->nei_s.p;
+    out->rev = c->nei_rev.p;
+    return HDNNP_OK;
 }
 
 // Device error flags of the last evaluation on c (valid after its stream has

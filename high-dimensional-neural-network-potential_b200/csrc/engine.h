@@ -200,6 +200,11 @@ struct PipePlan {
     double* pos_ref = nullptr;
 };
 
+// Device neighbour-list arrays of a context (ctx_list_arrays in capi.cu).
+struct CtxLists {
+    int *elem, *cnt, *off, *nj, *ns, *rev;
+};
+
 // Committee of potentials (committee.cu; globalHdnnpEnergyAndForces,
 // globalHdnnps.f90:31-70): neighbour lists and symmetry functions of the
 // first member, every member's networks on them; dE/dG is averaged before the

@@ -46,7 +46,9 @@ int model_device(const hdnnp_model* m);
 int set_error(int code, const std::string& msg);
 int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* Z_dev, const double* pos_dev,
                   const double* const* mol_pos, const int32_t* periodic, const double* lat, double* energy_dev,
-                  double* force_dev, double* dEdLat_dev, cudaStream_t st);
+                  double* force_dev, double* dEdLat_dev, cudaStream_t st, PipePlan* pp = nullptr,
+                  double rc_list = 0.0);
+int ctx_list_arrays(hdnnp_ctx* c, size_t natoms, size_t nentries, CtxLists* out);
 int ctx_check_status(hdnnp_ctx* c);
 int ctx_bad_struct(hdnnp_ctx* c);
 }  // namespace hdnnp
@@ -72,6 +74,21 @@ struct Walker {
     bool md = false, busy = false;
     unsigned long long steps = 0;
     size_t bytes = 0;
+    // Verlet-skin list (server option skin > 0): the walker's own CSR list
+    // (atom and entry indices local to the walker), the wrap translation and
+    // the positions of its last build
+    int *l_off = nullptr, *l_cnt = nullptr, *l_elem = nullptr, *l_j = nullptr, *l_s = nullptr, *l_rev = nullptr;
+    double *l_wsh = nullptr, *l_pref = nullptr;
+    int l_entries = 0, l_cap = 0, l_mmax = 0;
+    bool l_valid = false;
+};
+
+// One walker of a batch for the skin-list kernels (blockIdx.y = walker).
+struct WRef {
+    const double* pos;  // the walker's current positions
+    int *off, *cnt, *elem, *j, *s, *rev;
+    double *wsh, *pref;
+    int nat, a0, e0;  // atoms, first atom and first entry in the batch
 };
 
 struct Request {
@@ -95,11 +112,21 @@ struct Worker {
     int32_t* Z = nullptr;
     double *E = nullptr, *F = nullptr, *L = nullptr;
     double *hE = nullptr, *hF = nullptr, *hL = nullptr, *hpos = nullptr;  // pinned staging
+    // skin lists: batch wrap translations and reference positions, rebuild
+    // flags (1 and 0), per-walker flags, list offsets read back, walker tables
+    double *wshift = nullptr, *pos_ref = nullptr;
+    int *flag1 = nullptr, *flag0 = nullptr, *d_flags = nullptr, *h_flags = nullptr, *h_off = nullptr;
+    WRef *d_ref = nullptr, *h_ref = nullptr;
 };
 
 // Device bytes per walker atom: positions, kept positions, momenta, forces,
 // kept forces, previous forces (3 doubles each), mass, Z.
 constexpr size_t kWalkerBytesPerAtom = 6 * 24 + 8 + 4;
+// With a skin, a walker also keeps its neighbour list: charged as 80 entries
+// of 12 B per atom plus the per-atom offsets, counts, elements, wrap
+// translations and reference positions.
+constexpr size_t kSkinBytesPerAtom = 80 * 12 + 12 + 48;
+constexpr int kOne = 1;
 
 }  // namespace
 
@@ -121,6 +148,7 @@ struct hdnnp_server {
     // statistics since the last reset
     std::vector<double> lat_ms;
     long long atoms_done = 0, batches = 0, batched_requests = 0;
+    std::atomic<long long> list_builds{0}, list_reuses{0};  // walker lists built / kept (skin > 0)
     Clock::time_point t_first, t_last;
     bool have_first = false;
 };
@@ -164,12 +192,85 @@ void fail_batch(hdnnp_server* s, const std::vector<uint64_t>& batch, std::vector
     s->cv_req.notify_all();
 }
 
+// ------------------------------------------------------------ skin lists
+// flags[q] = 1 if an atom of walker q moved by more than sqrt(thr2) since its
+// list was built (or is not finite)
+__global__ void k_walker_moved(const WRef* t, double thr2, int* flags) {
+    const WRef w = t[blockIdx.y];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w.nat) return;
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double x = w.pos[3 * i + d] - w.pref[3 * i + d];
+        d2 += x * x;
+    }
+    if (!(d2 <= thr2)) atomicOr(&flags[blockIdx.y], 1);
+}
+
+// The batch's lists of walker q (just built) into the walker's storage,
+// indices made local.
+__global__ void k_lists_out(const WRef* t, CtxLists L, const double* wsh, const double* pref) {
+    const WRef w = t[blockIdx.y];
+    const int la = blockIdx.x * blockDim.x + threadIdx.x;
+    if (la >= w.nat) return;
+    const int a = w.a0 + la;
+    w.cnt[la] = L.cnt[a];
+    w.elem[la] = L.elem[a];
+    w.off[la] = L.off[a] - w.e0;
+    if (la == w.nat - 1) w.off[w.nat] = L.off[a + 1] - w.e0;
+    for (int d = 0; d < 3; ++d) {
+        w.wsh[3 * la + d] = wsh[3 * a + d];
+        w.pref[3 * la + d] = pref[3 * a + d];
+    }
+    for (int e = L.off[a]; e < L.off[a + 1]; ++e) {
+        const int le = e - w.e0;
+        w.j[le] = L.nj[e] - w.a0;
+        w.s[le] = L.ns[e];
+        w.rev[le] = L.rev[e] - w.e0;
+    }
+}
+
+// Walker q's kept list into the batch arrays at its atom and entry offsets.
+__global__ void k_lists_in(const WRef* t, CtxLists L, double* wsh, double* pref) {
+    const WRef w = t[blockIdx.y];
+    const int la = blockIdx.x * blockDim.x + threadIdx.x;
+    if (la >= w.nat) return;
+    const int a = w.a0 + la;
+    L.cnt[a] = w.cnt[la];
+    L.elem[a] = w.elem[la];
+    for (int d = 0; d < 3; ++d) {
+        wsh[3 * a + d] = w.wsh[3 * la + d];
+        pref[3 * a + d] = w.pref[3 * la + d];
+    }
+    for (int le = w.off[la]; le < w.off[la + 1]; ++le) {
+        const int e = w.e0 + le;
+        L.nj[e] = w.j[le] + w.a0;
+        L.ns[e] = w.s[le];
+        L.rev[e] = w.rev[le] + w.e0;
+    }
+}
+
+dim3 walker_grid(const std::vector<std::pair<Request*, Walker*>>& items) {
+    int nmax = 1;
+    for (auto& it : items) nmax = std::max(nmax, it.second->nat);
+    return dim3((unsigned)blocks(nmax), (unsigned)items.size());
+}
+
+enum class ListMode { Build, BuildKeep, Keep };
+
 // Evaluates the walkers of `items` (pre-step kernels already queued) as one
 // batch on the worker's stream: gather into the batch arrays, batched
 // pipeline, post-step (MD kick or force copy into the walker), results into
-// the requests.  Returns the batch status (message in `err`).
-int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, std::string& err) {
+// the requests.  Returns the batch status (message in `err`).  With a skin,
+// BuildKeep builds lists with cutoff rc + skin and keeps them in the walkers,
+// Keep evaluates on the walkers' kept lists.
+int evaluate_set(hdnnp_server* srv, Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, std::string& err,
+                 ListMode mode, int ab, int sb) {
+    // this part's walker table: entries sb.. (the other part's copy may be in flight)
     cudaStream_t st = w.stream;
+    double* bpos = w.pos + 3 * (size_t)ab;
+    int32_t* bZ = w.Z + ab;
+    double* bhpos = w.hpos + 3 * (size_t)ab;
     const size_t n = items.size();
     std::vector<int64_t> off(n + 1, 0);
     std::vector<int32_t> per(n);
@@ -181,12 +282,12 @@ int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, 
         off[q + 1] = off[q] + wk.nat;
         per[q] = wk.periodic;
         std::memcpy(&lat[9 * q], wk.lat, sizeof wk.lat);
-        cudaMemcpyAsync(w.pos + 3 * off[q], wk.pos, 24 * (size_t)wk.nat, cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(w.Z + off[q], wk.Z, 4 * (size_t)wk.nat, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(bpos + 3 * off[q], wk.pos, 24 * (size_t)wk.nat, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(bZ + off[q], wk.Z, 4 * (size_t)wk.nat, cudaMemcpyDeviceToDevice, st);
         if (!wk.periodic) {
             // a molecule's cell grid spans its bounding box: its positions come to the host
-            cudaMemcpyAsync(w.hpos + 3 * off[q], wk.pos, 24 * (size_t)wk.nat, cudaMemcpyDeviceToHost, st);
-            mol[q] = w.hpos + 3 * off[q];
+            cudaMemcpyAsync(bhpos + 3 * off[q], wk.pos, 24 * (size_t)wk.nat, cudaMemcpyDeviceToHost, st);
+            mol[q] = bhpos + 3 * off[q];
             have_mol = true;
         }
     }
@@ -195,8 +296,48 @@ int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, 
         err = cudaGetErrorString(ce);
         return HDNNP_E_CUDA;
     }
-    int status = eval_resident(w.ctx, (int)n, off.data(), w.Z, w.pos, mol.data(), per.data(), lat.data(), w.E, w.F,
-                               w.L, st);
+    const double skin = srv->opts.skin;
+    double rc_list = 0.0;
+    PipePlan pp{};
+    PipePlan* ppp = nullptr;
+    if (mode != ListMode::Build) {
+        int nel = 0, zs[128], ns[128];
+        double max_rc = 0;
+        hdnnp_model_info(srv->model, &nel, zs, ns, &max_rc);
+        rc_list = max_rc + skin;
+        pp.rc_list = rc_list;
+        pp.wshift = w.wshift;
+        pp.pos_ref = w.pos_ref;
+        ppp = &pp;
+    }
+    if (mode == ListMode::BuildKeep) {
+        pp.rebuild = w.flag1;  // build, recording the wrap translations and reference positions
+    } else if (mode == ListMode::Keep) {
+        // the walkers' lists into the batch arrays
+        long long ent = 0;
+        int mmax = 0;
+        for (size_t q = 0; q < n; ++q) {
+            const Walker& wk = *items[q].second;
+            w.h_ref[sb + q] = WRef{nullptr, wk.l_off, wk.l_cnt, wk.l_elem, wk.l_j, wk.l_s, wk.l_rev, wk.l_wsh, wk.l_pref,
+                              wk.nat, (int)off[q], (int)ent};
+            ent += wk.l_entries;
+            mmax = std::max(mmax, wk.l_mmax);
+        }
+        if (ent > INT32_MAX) return set_error(HDNNP_E_CAPACITY, "more than 2^31 neighbour entries in a batch");
+        CtxLists L{};
+        int r = ctx_list_arrays(w.ctx, (size_t)off[n], (size_t)ent, &L);
+        if (r) {
+            err = hdnnp_last_error();
+            return r;
+        }
+        cudaMemcpyAsync(w.d_ref + sb, w.h_ref + sb, sizeof(WRef) * n, cudaMemcpyHostToDevice, st);
+        k_lists_in<<<walker_grid(items), kThreads, 0, st>>>(w.d_ref + sb, L, w.wshift, w.pos_ref);
+        pp.rebuild = w.flag0;
+        pp.e_cap = ent;
+        pp.m_cap = std::max(32, (mmax + 31) / 32 * 32);
+    }
+    int status = eval_resident(w.ctx, (int)n, off.data(), bZ, bpos, mol.data(), per.data(), lat.data(), w.E + sb,
+                               w.F + 3 * (size_t)ab, w.L + 9 * (size_t)sb, st, ppp, rc_list);
     if (status) {
         err = hdnnp_last_error();
         cudaStreamSynchronize(st);
@@ -211,6 +352,68 @@ int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, 
         err = hdnnp_last_error();
         return status;
     }
+    if (mode == ListMode::BuildKeep) {
+        // keep each walker's new list: offsets to the host, storage, copy-out
+        CtxLists L{};
+        int r = ctx_list_arrays(w.ctx, (size_t)off[n], 0, &L);
+        if (r) {
+            err = hdnnp_last_error();
+            return r;
+        }
+        cudaMemcpyAsync(w.h_off, L.off, sizeof(int) * (size_t)(off[n] + 1), cudaMemcpyDeviceToHost, st);
+        if ((ce = cudaStreamSynchronize(st)) != cudaSuccess) {
+            err = cudaGetErrorString(ce);
+            return HDNNP_E_CUDA;
+        }
+        for (size_t q = 0; q < n; ++q) {
+            Walker& wk = *items[q].second;
+            const int e0 = w.h_off[off[q]], e1 = w.h_off[off[q + 1]];
+            int mmax = 0;
+            for (int64_t a = off[q]; a < off[q + 1]; ++a) mmax = std::max(mmax, w.h_off[a + 1] - w.h_off[a]);
+            const int ne = e1 - e0;
+            const size_t n3 = 3 * (size_t)wk.nat;
+            bool ok = true;
+            if (!wk.l_off)
+                ok = cudaMalloc(&wk.l_off, 4 * ((size_t)wk.nat + 1)) == cudaSuccess &&
+                     cudaMalloc(&wk.l_cnt, 4 * (size_t)wk.nat) == cudaSuccess &&
+                     cudaMalloc(&wk.l_elem, 4 * (size_t)wk.nat) == cudaSuccess &&
+                     cudaMalloc(&wk.l_wsh, 8 * n3) == cudaSuccess && cudaMalloc(&wk.l_pref, 8 * n3) == cudaSuccess;
+            if (ok && ne > wk.l_cap) {
+                for (int* p : {wk.l_j, wk.l_s, wk.l_rev})
+                    if (p) cudaFree(p);
+                wk.l_j = wk.l_s = wk.l_rev = nullptr;
+                wk.l_cap = ne + ne / 4 + 64;
+                ok = cudaMalloc(&wk.l_j, 4 * (size_t)wk.l_cap) == cudaSuccess &&
+                     cudaMalloc(&wk.l_s, 4 * (size_t)wk.l_cap) == cudaSuccess &&
+                     cudaMalloc(&wk.l_rev, 4 * (size_t)wk.l_cap) == cudaSuccess;
+            }
+            if (!ok) {
+                err = "skin-list storage could not be allocated";
+                return HDNNP_E_CUDA;
+            }
+            wk.l_entries = ne;
+            wk.l_mmax = mmax;
+            w.h_ref[sb + q] = WRef{nullptr, wk.l_off, wk.l_cnt, wk.l_elem, wk.l_j, wk.l_s, wk.l_rev, wk.l_wsh, wk.l_pref,
+                              wk.nat, (int)off[q], e0};
+        }
+        cudaMemcpyAsync(w.d_ref + sb, w.h_ref + sb, sizeof(WRef) * n, cudaMemcpyHostToDevice, st);
+        k_lists_out<<<walker_grid(items), kThreads, 0, st>>>(w.d_ref + sb, L, w.wshift, w.pos_ref);
+        for (auto& it : items) it.second->l_valid = true;
+        srv->list_builds += (long long)n;
+    } else if (mode == ListMode::Keep) {
+        srv->list_reuses += (long long)n;
+    }
+    return HDNNP_OK;
+}
+
+// Post-steps (MD kick or force copy into the walker) and results of the
+// walkers of `items`, evaluated from atom ab and structure sb of the batch
+// buffers; the whole batch's results come to the host at once.
+int finish_batch(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, std::string& err) {
+    cudaStream_t st = w.stream;
+    const size_t n = items.size();
+    std::vector<int64_t> off(n + 1, 0);
+    for (size_t q = 0; q < n; ++q) off[q + 1] = off[q] + items[q].second->nat;
     for (size_t q = 0; q < n; ++q) {
         const Request& r = *items[q].first;
         Walker& wk = *items[q].second;
@@ -223,6 +426,7 @@ int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, 
     cudaMemcpyAsync(w.hE, w.E, 8 * n, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(w.hF, w.F, 24 * (size_t)off[n], cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(w.hL, w.L, 72 * n, cudaMemcpyDeviceToHost, st);
+    cudaError_t ce;
     if ((ce = cudaStreamSynchronize(st)) != cudaSuccess) {
         err = cudaGetErrorString(ce);
         return HDNNP_E_CUDA;
@@ -234,6 +438,67 @@ int evaluate(Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, 
         std::memcpy(r.dEdLat, w.hL + 9 * q, sizeof r.dEdLat);
     }
     return HDNNP_OK;
+}
+
+// Without a skin: one batch.  With a skin: walkers whose atoms all stayed
+// within skin/2 of their list's reference positions are evaluated on their
+// kept lists, the others (and walkers without a list) build new ones -- two
+// pipeline runs at most, each batched over its walkers, into separate parts
+// of the batch buffers; post-steps only once both have succeeded.  On
+// failure *bad names the item whose input the device flags blame, or -1.
+int evaluate(hdnnp_server* srv, Worker& w, const std::vector<std::pair<Request*, Walker*>>& items, std::string& err,
+             int* bad) {
+    *bad = -1;
+    using Items = std::vector<std::pair<Request*, Walker*>>;
+    auto blame = [&](const Items& part) {
+        const int k = ctx_bad_struct(w.ctx);
+        if (k >= 0 && k < (int)part.size())
+            for (size_t q = 0; q < items.size(); ++q)
+                if (items[q].second == part[k].second) *bad = (int)q;
+    };
+    int r;
+    if (!(srv->opts.skin > 0.0) || items.size() > 65535) {
+        // (the skin-list kernels index walkers by grid y, at most 65535)
+        if ((r = evaluate_set(srv, w, items, err, ListMode::Build, 0, 0))) {
+            blame(items);
+            return r;
+        }
+        return finish_batch(w, items, err);
+    }
+    cudaStream_t st = w.stream;
+    Items keep, build, cand;
+    for (auto& it : items) (it.second->l_valid ? cand : build).push_back(it);
+    if (!cand.empty()) {
+        for (size_t q = 0; q < cand.size(); ++q) {
+            const Walker& wk = *cand[q].second;
+            w.h_ref[q] = WRef{wk.pos, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, wk.l_pref,
+                              wk.nat, 0, 0};
+        }
+        cudaMemcpyAsync(w.d_ref, w.h_ref, sizeof(WRef) * cand.size(), cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(w.d_flags, 0, sizeof(int) * cand.size(), st);
+        const double half = 0.5 * srv->opts.skin;
+        k_walker_moved<<<walker_grid(cand), kThreads, 0, st>>>(w.d_ref, half * half, w.d_flags);
+        cudaMemcpyAsync(w.h_flags, w.d_flags, sizeof(int) * cand.size(), cudaMemcpyDeviceToHost, st);
+        const cudaError_t ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) {
+            err = cudaGetErrorString(ce);
+            return HDNNP_E_CUDA;
+        }
+        for (size_t q = 0; q < cand.size(); ++q) (w.h_flags[q] ? build : keep).push_back(cand[q]);
+    }
+    int nb_atoms = 0;
+    for (auto& it : build) nb_atoms += it.second->nat;
+    if (!build.empty() && (r = evaluate_set(srv, w, build, err, ListMode::BuildKeep, 0, 0))) {
+        blame(build);
+        return r;
+    }
+    if (!keep.empty() && (r = evaluate_set(srv, w, keep, err, ListMode::Keep, nb_atoms, (int)build.size()))) {
+        blame(keep);
+        return r;
+    }
+    Items all(build);
+    all.insert(all.end(), keep.begin(), keep.end());
+    return finish_batch(w, all, err);
 }
 
 void process_batch(hdnnp_server* s, Worker& w, const std::vector<uint64_t>& batch) {
@@ -277,9 +542,9 @@ void process_batch(hdnnp_server* s, Worker& w, const std::vector<uint64_t>& batc
         // the walker named by the device flags leaves the batch and the rest
         // is evaluated again; without a name each walker is evaluated alone.
         while (!ev.empty()) {
-            status = evaluate(w, ev, err);
+            int bad = -1;
+            status = evaluate(s, w, ev, err, &bad);
             if (status != HDNNP_E_INPUT && status != HDNNP_E_CAPACITY) break;
-            const int bad = ctx_bad_struct(w.ctx);
             if (ev.size() == 1) {
                 ev[0].first->status = status;
                 ev[0].first->err = err;
@@ -295,7 +560,8 @@ void process_batch(hdnnp_server* s, Worker& w, const std::vector<uint64_t>& batc
             status = HDNNP_OK;
             for (auto& it : ev) {
                 std::string e1;
-                it.first->status = evaluate(w, {it}, e1);
+                int b1 = -1;
+                it.first->status = evaluate(s, w, {it}, e1, &b1);
                 it.first->err = e1;
                 if (it.first->status == HDNNP_E_CUDA) {
                     status = HDNNP_E_CUDA;
@@ -379,7 +645,8 @@ void worker_loop(hdnnp_server* s, Worker* w) {
 
 void free_walker(Walker& w) {
     for (void* p : {(void*)w.pos, (void*)w.pos_keep, (void*)w.mom, (void*)w.mass, (void*)w.force,
-                    (void*)w.force_keep, (void*)w.force_prev, (void*)w.Z})
+                    (void*)w.force_keep, (void*)w.force_prev, (void*)w.Z, (void*)w.l_off, (void*)w.l_cnt,
+                    (void*)w.l_elem, (void*)w.l_j, (void*)w.l_s, (void*)w.l_rev, (void*)w.l_wsh, (void*)w.l_pref})
         if (p) cudaFree(p);
 }
 
@@ -394,6 +661,7 @@ int hdnnp_server_create(hdnnp_model* m, const hdnnp_server_opts* opts, hdnnp_ser
     if (opts->max_batch_atoms < 1) return set_error(HDNNP_E_INPUT, "max_batch_atoms must be positive");
     if (opts->precision != HDNNP_PREC_FP64 && opts->precision != HDNNP_PREC_MIXED)
         return set_error(HDNNP_E_INPUT, "unknown precision");
+    if (!(opts->skin >= 0.0) || !std::isfinite(opts->skin)) return set_error(HDNNP_E_INPUT, "skin must be finite and >= 0");
     const size_t ws = (size_t)opts->workers * opts->max_batch_atoms * workspace_bytes_per_atom(m);
     if (opts->hbm_budget && ws > opts->hbm_budget)
         return set_error(HDNNP_E_CAPACITY, "HBM budget (" + std::to_string(opts->hbm_budget) +
@@ -419,7 +687,17 @@ int hdnnp_server_create(hdnnp_model* m, const hdnnp_server_opts* opts, hdnnp_ser
                         cudaMallocHost(&w.hF, na * 24) == cudaSuccess &&
                         cudaMallocHost(&w.hL, na * 72) == cudaSuccess &&
                         cudaMallocHost(&w.hpos, na * 24) == cudaSuccess;
-        if (!ok) {
+        const bool ok2 = !ok || !(opts->skin > 0.0) ||
+                         (cudaMalloc(&w.wshift, na * 24) == cudaSuccess && cudaMalloc(&w.pos_ref, na * 24) == cudaSuccess &&
+                          cudaMalloc(&w.flag1, 4) == cudaSuccess && cudaMalloc(&w.flag0, 4) == cudaSuccess &&
+                          cudaMemcpy(w.flag1, &kOne, 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                          cudaMemset(w.flag0, 0, 4) == cudaSuccess &&
+                          cudaMalloc(&w.d_flags, 4 * na) == cudaSuccess &&
+                          cudaMallocHost(&w.h_flags, 4 * na) == cudaSuccess &&
+                          cudaMallocHost(&w.h_off, 4 * (na + 1)) == cudaSuccess &&
+                          cudaMalloc(&w.d_ref, sizeof(WRef) * na) == cudaSuccess &&
+                          cudaMallocHost(&w.h_ref, sizeof(WRef) * na) == cudaSuccess);
+        if (!ok || !ok2) {
             std::string msg = r ? std::string(hdnnp_last_error()) : "server buffers could not be allocated";
             hdnnp_server_destroy(s);
             return set_error(r ? r : HDNNP_E_CUDA, msg);
@@ -442,9 +720,11 @@ void hdnnp_server_destroy(hdnnp_server* s) {
     cudaSetDevice(s->device);
     for (auto& w : s->workers) {
         if (w.stream) cudaStreamSynchronize(w.stream);
-        for (void* p : {(void*)w.pos, (void*)w.Z, (void*)w.E, (void*)w.F, (void*)w.L})
+        for (void* p : {(void*)w.pos, (void*)w.Z, (void*)w.E, (void*)w.F, (void*)w.L, (void*)w.wshift,
+                        (void*)w.pos_ref, (void*)w.flag1, (void*)w.flag0, (void*)w.d_flags, (void*)w.d_ref})
             if (p) cudaFree(p);
-        for (void* p : {(void*)w.hE, (void*)w.hF, (void*)w.hL, (void*)w.hpos})
+        for (void* p : {(void*)w.hE, (void*)w.hF, (void*)w.hL, (void*)w.hpos, (void*)w.h_flags, (void*)w.h_off,
+                        (void*)w.h_ref})
             if (p) cudaFreeHost(p);
         if (w.stream) cudaStreamDestroy(w.stream);
         if (w.ctx) hdnnp_ctx_free(w.ctx);
@@ -471,7 +751,7 @@ int hdnnp_server_add_walker(hdnnp_server* s, int nat, const int32_t* Z, const do
     if (masses)
         for (int i = 0; i < nat; ++i)
             if (!(masses[i] > 0)) return set_error(HDNNP_E_INPUT, "masses must be positive");
-    const size_t bytes = (size_t)nat * kWalkerBytesPerAtom;
+    const size_t bytes = (size_t)nat * (kWalkerBytesPerAtom + (s->opts.skin > 0.0 ? kSkinBytesPerAtom : 0));
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (s->opts.hbm_budget && s->hbm_walkers + bytes + s->hbm_workspace > s->opts.hbm_budget)
@@ -605,6 +885,13 @@ int hdnnp_server_read_walker(hdnnp_server* s, int walker, double* pos, double* m
         return set_error(HDNNP_E_CUDA, "walker position copy failed");
     if (momenta && cudaMemcpy(momenta, w.mom, 24 * (size_t)w.nat, cudaMemcpyDeviceToHost) != cudaSuccess)
         return set_error(HDNNP_E_CUDA, "walker momentum copy failed");
+    return HDNNP_OK;
+}
+
+int hdnnp_server_list_stats(hdnnp_server* s, int64_t* built, int64_t* kept) {
+    if (!s) return set_error(HDNNP_E_INPUT, "null server");
+    if (built) *built = s->list_builds.load();
+    if (kept) *kept = s->list_reuses.load();
     return HDNNP_OK;
 }
 

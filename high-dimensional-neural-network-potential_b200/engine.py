@@ -89,6 +89,7 @@ def lib():
     L.hdnnp_server_next_done.argtypes = [P, C.c_int, C.POINTER(C.c_uint64)]
     L.hdnnp_server_read_walker.argtypes = [P, C.c_int, D, D]
     L.hdnnp_server_stats.argtypes = [P, D, D, D, D, C.POINTER(C.c_size_t), C.c_int]
+    L.hdnnp_server_list_stats.argtypes = [P, I64, I64]
     _lib = L
     return L
 

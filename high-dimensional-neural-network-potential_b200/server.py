@@ -32,14 +32,16 @@ E_TIMEOUT = 4
 
 class _Opts(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_batch_atoms", C.c_int), ("workers", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("skin", C.c_double)]
 
 
 class Server:
     def __init__(self, pot, max_batch_atoms: int = 65536, workers: int = 2, precision: int = HDNNP_PREC_FP64,
-                 hbm_budget: int = 0):
+                 hbm_budget: int = 0, skin: float = 0.0):
+        """skin > 0 (Bohr): walkers keep their neighbour lists (cutoff rc + skin)
+        and build them again only after an atom moved by more than skin/2."""
         self._pot = pot  # keeps the model alive
-        o = _Opts(int(hbm_budget), int(max_batch_atoms), int(workers), int(precision))
+        o = _Opts(int(hbm_budget), int(max_batch_atoms), int(workers), int(precision), float(skin))
         h = C.c_void_p()
         _check(lib().hdnnp_server_create(pot._m, C.byref(o), C.byref(h)))
         self._s = h
@@ -131,6 +133,12 @@ class Server:
         _check(lib().hdnnp_server_stats(self._s, *[C.byref(x) for x in v], C.byref(hbm), 1 if reset else 0))
         return {"p50_ms": v[0].value, "p99_ms": v[1].value, "atom_steps_per_s": v[2].value,
                 "mean_batch_requests": v[3].value, "hbm_charged": hbm.value}
+
+    def list_stats(self) -> dict:
+        """Walker neighbour lists built and kept so far (skin > 0)."""
+        b, k = C.c_int64(), C.c_int64()
+        _check(lib().hdnnp_server_list_stats(self._s, C.byref(b), C.byref(k)))
+        return {"built": b.value, "kept": k.value}
 
 
 def poisson_load(srv: Server, walkers, rate: Optional[float], duration: float, seed: int = 0, sigma: float = 0.05,

@@ -275,6 +275,12 @@ typedef struct {
     int max_batch_atoms; /* atom slots of one batch (also the largest walker)    */
     int workers;         /* concurrent batches, 1..8                             */
     int precision;       /* HDNNP_PREC_FP64 or HDNNP_PREC_MIXED                  */
+    double skin;         /* Verlet skin (Bohr) of the walkers' neighbour lists; 0:
+                            lists are built for every request.  With a skin each
+                            walker keeps its list (cutoff rc + skin) and builds
+                            it again only when one of its atoms has moved by more
+                            than skin/2 since; a batch evaluates its walkers that
+                            need a list and those that keep one as two parts    */
 } hdnnp_server_opts;
 
 typedef enum {
@@ -320,6 +326,11 @@ int hdnnp_server_read_walker(hdnnp_server* s, int walker, double* pos, double* m
  * and HBM bytes charged to walkers + workspaces.  reset != 0 clears them.    */
 int hdnnp_server_stats(hdnnp_server* s, double* p50_ms, double* p99_ms, double* atom_steps_per_s,
                        double* mean_batch_requests, size_t* hbm_charged, int reset);
+
+/* Walker neighbour lists built and kept since the server started (skin > 0;
+ * both 0 otherwise).  No reference counterpart: the reference builds the
+ * lists on every call (hdnnps.f90:347).                                      */
+int hdnnp_server_list_stats(hdnnp_server* s, int64_t* built, int64_t* kept);
 
 #ifdef __cplusplus
 }

@@ -300,3 +300,46 @@ def test_failing_walker_fails_alone(pot, S, W, abx3_model):
             assert abs(E - ref["energy"]) <= RTOL_E * abs(ref["energy"])
             assert np.abs(F - ref["forces"]).max() <= ATOL_F
         assert srv.stats()["mean_batch_requests"] > 1.0
+
+
+def test_skin_lists_match_rebuilt_lists(pot, S, W):
+    """Walkers that keep their neighbour lists (skin 1 Bohr) follow the same
+    trajectories as walkers whose lists are rebuilt for every request (FP64,
+    within summation-order rounding), in batches that mix walkers keeping
+    and rebuilding lists: MD walkers move little per step and keep theirs,
+    Monte Carlo trials of sigma 0.6 Bohr every third step force rebuilds."""
+    walkers = small_walkers(W, 6, 61)
+    mol = W.abx3_cell()
+    walkers.append({"Z": mol["Z"], "pos": mol["pos"] + 4.0, "lat": None})
+    kw = dict(max_batch_atoms=4096, workers=1, precision=0)
+    with S.Server(pot, **kw) as a, S.Server(pot, skin=1.0, **kw) as b:
+        ids = []
+        for k, s in enumerate(walkers):
+            md = k % 2 == 0
+            m, p = W.maxwell_boltzmann(s["Z"], 300.0, 70 + k) if md else (None, None)
+            ids.append((a.add_walker(s["Z"], s["pos"], s["lat"], masses=m, momenta=p),
+                        b.add_walker(s["Z"], s["pos"], s["lat"], masses=m, momenta=p), md))
+        evals = 0
+        for step in range(10):
+            ta, tb = [], []
+            for k, (wa, wb, md) in enumerate(ids):
+                if step == 0:
+                    args = dict(kind=S.REQ_EVAL)
+                elif md:
+                    args = dict(kind=S.REQ_MD_STEP, dt=0.5)
+                else:
+                    args = dict(kind=S.REQ_MC_TRIAL, sigma=0.6 if step % 3 == 0 else 0.02, seed=1000 * step + k)
+                ta.append(a.submit(wa, **args))
+                tb.append(b.submit(wb, **args))
+            for x, y in zip(ta, tb):
+                Ea, Fa, La, _ = a.wait(x)
+                Eb, Fb, Lb, _ = b.wait(y)
+                assert abs(Ea - Eb) <= 1e-10 * abs(Ea)
+                assert np.abs(Fa - Fb).max() <= 1e-9
+                assert np.abs(La - Lb).max() <= 1e-9
+                evals += 1
+        st = b.list_stats()
+        print("skin lists:", st, "evaluations", evals)
+        assert st["built"] + st["kept"] == evals
+        assert st["kept"] > 0 and len(walkers) < st["built"] < evals
+        assert a.list_stats() == {"built": 0, "kept": 0}
