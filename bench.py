@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="seconds per load point of the serving leg (0: skip)")
     ap.add_argument("--md", type=int, default=1, help="1: run the device-resident MD legs")
+    ap.add_argument("--only-leg", choices=["c1", "c2", "c3"], default=None,
+                    help="run one single-structure leg alone (C1 example MD, C2 768-atom cell, C3 49,152-atom MD) "
+                         "and print its JSON: for profiling")
     ap.add_argument("--lean", action="store_true",
                     help="device-resident steps only (no e2e, comparisons, peaks or CPU baseline): for profiler runs")
     return ap.parse_args()
@@ -291,7 +294,7 @@ def serve_leg(pkg, engine, pot, prec, seconds):
             "saturation": sat, "poisson_sweep": sweep}
 
 
-def md_legs(pkg, engine, PLm, pot, torch):
+def md_legs(pkg, engine, PLm, pot, torch, which=("c1", "c2", "c3")):
     """The single-structure workloads, each with the CPU stand-in (the oracle
     on all host threads) timed beside it.
 
@@ -321,6 +324,21 @@ def md_legs(pkg, engine, PLm, pot, torch):
         builds = plan.sync(st.cuda_stream)
         return e0.elapsed_time(e1) / 1e3, builds
 
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    if "c1" in which:
+        out.update(leg_c1(W, engine, PLm, timed))
+    if "c2" in which:
+        out.update(leg_c2(W, engine, PLm, pot, timed, O))
+    if "c3" in which:
+        out.update(leg_c3(W, engine, PLm, pot, timed, O))
+    return out
+
+
+def leg_c1(W, engine, PLm, timed):
+    """C1: the reference's example molecule, MD on the device vs the plain API and the CPU oracle."""
+    out = {}
     s, m, p0 = W.config_c1(EXAMPLE_DIR)
     pot1 = engine.Hdnnp.from_runner(EXAMPLE_DIR)
     pl = PLm.Plan(pot1, [s], masses=m, momenta=p0, dt=20.0, steps_per_launch=100, want_dEdLat=False)
@@ -367,8 +385,12 @@ def md_legs(pkg, engine, PLm, pot, torch):
         "cpu_oracle_steps_per_s": 1000 / csec, "cpu_cores": O.max_threads()}
     pl.close()
     pot1.close()
+    return out
 
-    # 768-atom cell: one structure per call (FP64 and mixed) and as a plan (graph)
+
+def leg_c2(W, engine, PLm, pot, timed, O):
+    """C2: the 768-atom cell, one structure per call (FP64 and mixed) and as a plan (graph)."""
+    out = {}
     s2 = W.config_c2()
     ats2 = engine.AtStruct(s2["Z"], s2["pos"], s2["lat"])
     c2 = {"workload": "768-atom ABX3 4x4x4 cell (seed 1), E+F+stress"}
@@ -397,7 +419,13 @@ def md_legs(pkg, engine, PLm, pot, torch):
     c2["cpu_oracle_ms"] = float(np.median(ts) * 1e3)
     c2["atom_steps_per_s"] = {k[:-3]: 768 / (v / 1e3) for k, v in c2.items() if k.endswith("_ms")}
     out["cell_768"] = c2
+    return out
 
+
+def leg_c3(W, engine, PLm, pot, timed, O):
+    """C3: the strained 49,152-atom cell, MD on the device with a 1 Bohr Verlet skin."""
+    out = {}
+    om2 = O.Model(POT_DIR)
     s3 = W.config_c3()
     m3, p3 = W.maxwell_boltzmann(s3["Z"], 300.0, 3)
     pl3 = PLm.Plan(pot, [s3], precision=engine.HDNNP_PREC_MIXED, skin=1.0, masses=m3, momenta=p3, dt=DT_SYNTH,
@@ -419,6 +447,7 @@ def md_legs(pkg, engine, PLm, pot, torch):
         "cpu_oracle_atom_steps_per_s": len(s3c["Z"]) / c3sec,
         "cpu_sample": f"8x8x8 cut ({len(s3c['Z'])} atoms), E+F+stress, FP64"}
     pl3.close()
+    pot.set_precision(engine.HDNNP_PREC_FP64)
     return out
 
 
@@ -442,6 +471,15 @@ def main():
     from hdnnp_b200 import engine
 
     W = pkg.workloads
+    if args.only_leg:
+        from hdnnp_b200 import plan as PLm
+
+        pot = engine.Hdnnp.from_runner(POT_DIR, device=local)
+        res = md_legs(pkg, engine, PLm, pot, torch, which=(args.only_leg,))
+        if rank == 0:
+            print(json.dumps({"leg": args.only_leg, **res}), flush=True)
+        pot.close()
+        return
     structs, off, Z, pos, per, latf = workload(W, args.structs, 4 + rank)
     natoms = int(off[-1])
     nstruct = len(structs)
