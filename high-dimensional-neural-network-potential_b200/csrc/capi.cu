@@ -445,7 +445,10 @@ int upload_model(hdnnp_model* m) {
                      szAb = (size_t)2 * 128 * kH * 2;
         // b1, then each later layer's W and bias zero-padded to kH x kH and kH
         const size_t wsmall = kH + (size_t)(L - 1) * (kH * kH + kH);
-        const size_t total = std::max(szA, szBb + szAb) + szBf + ((wsmall * 4 + 15) & ~size_t(15)) + 64;
+        // (after GEMM 1 the A_fwd region holds B_bwd, A_bwd and the hidden
+        // layers' activation exchange, two 128 x kH FP32 buffers)
+        const size_t total = std::max(szA, szBb + szAb + (size_t)2 * 128 * kH * 4) + szBf +
+                             ((wsmall * 4 + 15) & ~size_t(15)) + 64;
         ok = ok && total <= 227 * 1024;
         if (ok) {
             auto cm = [](int row, int k, int rows) {

@@ -31,7 +31,10 @@ namespace hdnnp {
 namespace {
 
 constexpr int kM = 128;        // atoms per tile (TMEM lanes, MMA M)
-constexpr int kThr = 128;      // threads per CTA (4 warps; thread = row)
+constexpr int kThr = 512;      // threads per CTA: 16 warps; warp w serves TMEM lanes (rows)
+                               // 32 (w % 4) .. +31 and quarter w / 4 of each layer's neurons
+constexpr int kQ = kThr / kM;  // threads per row (4)
+constexpr int kHq = 32 / kQ;   // neurons of a padded layer per thread (8)
 constexpr int kH = 32;         // padded hidden width (N of GEMM 1, K of GEMM 2)
 constexpr int kTmemCols = 512;
 constexpr long long kWaitIters = 1LL << 22;
@@ -151,7 +154,9 @@ __host__ __device__ inline TCPlan tc_plan(const DevModel& m) {
     p.szAb = (size_t)2 * kM * kH * 2;
     const size_t w = kH + (size_t)(m.nlayers - 1) * (kH * kH + kH);  // b1, then W_l and b_l padded
     p.szW = ((w * 4) + 15) & ~size_t(15);
-    size_t reuse = p.szBb + p.szAb;
+    // the A_fwd region after GEMM 1: B_bwd | A_bwd, then the activation
+    // exchange of the hidden layers (two [kM][kH] FP32 buffers)
+    size_t reuse = p.szBb + p.szAb + (size_t)2 * kM * kH * 4;
     p.total = (p.szA > reuse ? p.szA : reuse) + p.szBf + p.szW + 64;
     return p;
 }
@@ -179,7 +184,8 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
     const int H = m.width[1];
     constexpr int L = NL;
     unsigned char* sA = sm;
-    unsigned char* sBf = sm + (P.szA > P.szBb + P.szAb ? P.szA : P.szBb + P.szAb);
+    const size_t reuse = P.szBb + P.szAb + (size_t)2 * kM * kH * 4;  // B_bwd | A_bwd | exchange
+    unsigned char* sBf = sm + (P.szA > reuse ? P.szA : reuse);
     float* sW = (float*)(sBf + P.szBf);
     uint64_t* mbar = (uint64_t*)((unsigned char*)sW + P.szW);
     uint32_t* tslot = (uint32_t*)(mbar + 1);
@@ -218,35 +224,37 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
             o += kH;
         }
     }
-    // ---- stage A_fwd: thread = row; its row of G' (FP32) -> FP16 hi | lo in
-    // groups of 4 k (one 8-byte store per part), zero padding.  32 values are
-    // loaded before any is stored, so each thread keeps 8 vector loads in flight.
+    // ---- stage A_fwd: thread (row, quarter q); its row of G' (FP32) -> FP16
+    // hi | lo in groups of 4 k (one 8-byte store per part), zero padding; the
+    // quarter takes every kQ-th block of 32 k.  32 values are loaded before
+    // any is stored, so each thread keeps 8 vector loads in flight.
+    const int row = (warp & 3) * 32 + (tid & 31), quarter = warp >> 2;
     {
         __half* Ahi = (__half*)sA;
         __half* Alo = (__half*)(sA + P.szA / 2);
         const int kp = P.Kp;
-        const int r = tid;
+        const int r = row;
         const int at = r < cnt ? b.el_atoms[t0 + r] : -1;
-        const float* row = at >= 0 ? b.Gf + (size_t)at * m.nsf_max : nullptr;
+        const float* grow = at >= 0 ? b.Gf + (size_t)at * m.nsf_max : nullptr;
         const bool vec = (m.nsf_max & 3) == 0;
-        for (int k0 = 0; k0 < kp; k0 += 32) {
+        for (int k0 = 32 * quarter; k0 < kp; k0 += 32 * kQ) {
             float x[32];
             if (vec && at >= 0) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int k = k0 + 4 * q;
                     float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (k + 3 < nin) f = *(const float4*)(row + k);
+                    if (k + 3 < nin) f = *(const float4*)(grow + k);
                     else {
-                        if (k < nin) f.x = row[k];
-                        if (k + 1 < nin) f.y = row[k + 1];
-                        if (k + 2 < nin) f.z = row[k + 2];
+                        if (k < nin) f.x = grow[k];
+                        if (k + 1 < nin) f.y = grow[k + 1];
+                        if (k + 2 < nin) f.z = grow[k + 2];
                     }
                     x[4 * q] = f.x; x[4 * q + 1] = f.y; x[4 * q + 2] = f.z; x[4 * q + 3] = f.w;
                 }
             } else {
 #pragma unroll
-                for (int q = 0; q < 32; ++q) x[q] = (at >= 0 && k0 + q < nin) ? row[k0 + q] : 0.f;
+                for (int q = 0; q < 32; ++q) x[q] = (at >= 0 && k0 + q < nin) ? grow[k0 + q] : 0.f;
             }
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -288,40 +296,62 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
     }
     ok = mbar_wait(mb, 0);
     tc_fence_after();
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;  // A_fwd is free from here on
 
-    const int row = tid;
     const bool live = row < cnt;
     const int atom = live ? b.el_atoms[t0 + row] : 0;
+    // activation exchange: two [kM][kH] buffers after B_bwd | A_bwd in the A_fwd region
+    float* xa = (float*)(sA + P.szBb + P.szAb);
+    float* xb = xa + kM * kH;
+    const int o0 = quarter * kHq;  // this thread's neurons o0 .. o0 + kHq - 1
     if (ok) {
-        // offsets of the padded FP32 weights of layers 1..L-1 in sW
         constexpr int kWB = kH * kH + kH;
         auto woff = [](int l) { return kH + (l - 1) * kWB; };
         auto boff = [](int l) { return kH + (l - 1) * kWB + kH * kH; };
         float v[32];
-        tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), v);
+        tmem_ld32(tbase + ((uint32_t)((warp & 3) * 32) << 16), v);
         const float inv = m.tc_inv_s1[e];
-        float yp[kH];          // activations of the previous layer
-        float dact[NL][kH];    // act'(c) of every layer, for the backward pass
+        float dact[NL][kHq];  // act'(c) of this thread's neurons of every layer
+        // first hidden layer: own neurons, activations to the exchange buffer
 #pragma unroll
-        for (int o = 0; o < kH; ++o) {
-            const float c = o < H ? v[o] * inv + sW[o] : 0.f;
-            const float yv = o < H ? act_fw(m.act[0], c) : 0.f;
-            yp[o] = yv;
-            dact[0][o] = o < H ? act_dv(m.act[0], c, yv) : 0.f;
+        for (int u = 0; u < kHq; ++u) {
+            const int o = o0 + u;
+            float c = 0.f, yv = 0.f, dv = 0.f;
+#pragma unroll
+            for (int qq = 0; qq < kQ; ++qq)  // v[o] with a compile-time index
+                if (qq == quarter) c = v[qq * kHq + u];
+            if (o < H) {
+                c = c * inv + sW[o];
+                yv = act_fw(m.act[0], c);
+                dv = act_dv(m.act[0], c, yv);
+            }
+            xa[row * kH + o] = yv;
+            dact[0][u] = dv;
         }
-        // Layers 2..L: the padded rows are read as float4 (broadcast: every
-        // thread reads the same weights); neurons beyond the layer's width
-        // are skipped by a branch uniform over the CTA.  Padding adds only
-        // zero terms, in the same order as the unpadded sums.
+        __syncthreads();
+        // Layers 2..L: each thread its neurons from the whole previous layer
+        // (read back from the exchange buffer); padded rows read as float4
+        // (broadcast), neurons beyond the layer's width skipped by a branch
+        // uniform over the CTA.  Padding adds only zero terms, in the same
+        // order as the unpadded sums.
+        float* cur = xa;
+        float* nxt = xb;
+        float yout = 0.f;  // output neuron (quarter 0)
 #pragma unroll
         for (int l = 1; l < NL; ++l) {
             const int wo = m.width[l + 1];
             const float4* W4 = (const float4*)(sW + woff(l));
             const float* bb = sW + boff(l);
             const char al = m.act[l];
-            float yc[kH];
+            float yp[kH];
 #pragma unroll
-            for (int o = 0; o < kH; ++o) {
+            for (int q = 0; q < kH / 4; ++q) {
+                const float4 t = *(const float4*)(cur + row * kH + 4 * q);
+                yp[4 * q] = t.x; yp[4 * q + 1] = t.y; yp[4 * q + 2] = t.z; yp[4 * q + 3] = t.w;
+            }
+#pragma unroll
+            for (int u = 0; u < kHq; ++u) {
+                const int o = o0 + u;
                 float c = 0.f, yv = 0.f, dv = 0.f;
                 if (o < wo) {
                     c = bb[o];
@@ -336,51 +366,76 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
                     yv = act_fw(al, c);
                     dv = act_dv(al, c, yv);
                 }
-                yc[o] = yv;
-                dact[l][o] = dv;
+                nxt[row * kH + o] = yv;
+                dact[l][u] = dv;
+                if (l == NL - 1 && o == 0) yout = yv;
             }
-#pragma unroll
-            for (int o = 0; o < kH; ++o) yp[o] = yc[o];
+            __syncthreads();
+            float* t = cur;
+            cur = nxt;
+            nxt = t;
         }
-        if (live) b.atEf[atom] = (float)((double)yp[0] + m.atom_energy[e]);
-        // backward (gradOut = 1) down to the first hidden layer
-        float d[kH];
+        if (live && quarter == 0) b.atEf[atom] = (float)((double)yout + m.atom_energy[e]);
+        // backward (gradOut = 1) down to the first hidden layer: deltas of
+        // this thread's neurons; the whole delta vector of a layer through
+        // the exchange buffer
 #pragma unroll
-        for (int o = 0; o < kH; ++o) d[o] = dact[NL - 1][o];
+        for (int u = 0; u < kHq; ++u) cur[row * kH + o0 + u] = dact[NL - 1][u];
+        __syncthreads();
+        float d[kHq];
 #pragma unroll
         for (int l = NL - 1; l >= 1; --l) {
             const int wo = m.width[l + 1];
             const float4* W4 = (const float4*)(sW + woff(l));
-            float g[kH];
+            float dl[kH];
 #pragma unroll
-            for (int i = 0; i < kH; ++i) g[i] = 0.f;
-            // g_i = sum over o (ascending) of W[o][i] d_o, four i per float4 row load
+            for (int q = 0; q < kH / 4; ++q) {
+                const float4 t = *(const float4*)(cur + row * kH + 4 * q);
+                dl[4 * q] = t.x; dl[4 * q + 1] = t.y; dl[4 * q + 2] = t.z; dl[4 * q + 3] = t.w;
+            }
+            float g[kHq];
+#pragma unroll
+            for (int u = 0; u < kHq; ++u) g[u] = 0.f;
+            // g_i = sum over o (ascending) of W[o][i] d_o, for this thread's i
 #pragma unroll
             for (int o = 0; o < kH; ++o) {
                 if (o < wo) {
 #pragma unroll
-                    for (int q = 0; q < kH / 4; ++q) {
-                        const float4 w = W4[o * (kH / 4) + q];
-                        g[4 * q] += w.x * d[o];
-                        g[4 * q + 1] += w.y * d[o];
-                        g[4 * q + 2] += w.z * d[o];
-                        g[4 * q + 3] += w.w * d[o];
+                    for (int q = 0; q < kHq / 4; ++q) {
+                        const float4 w = W4[o * (kH / 4) + quarter * (kHq / 4) + q];
+                        g[4 * q] += w.x * dl[o];
+                        g[4 * q + 1] += w.y * dl[o];
+                        g[4 * q + 2] += w.z * dl[o];
+                        g[4 * q + 3] += w.w * dl[o];
                     }
                 }
             }
 #pragma unroll
-            for (int i = 0; i < kH; ++i) d[i] = g[i] * dact[l - 1][i];
+            for (int u = 0; u < kHq; ++u) d[u] = g[u] * dact[l - 1][u];
+            if (l > 1) {
+#pragma unroll
+                for (int u = 0; u < kHq; ++u) nxt[row * kH + o0 + u] = d[u];
+                __syncthreads();
+                float* t = cur;
+                cur = nxt;
+                nxt = t;
+            }
         }
-        // ---- stage A_bwd (delta1 scaled, hi | lo) and B_bwd in the A_fwd region
+        if (NL == 1) {
+#pragma unroll
+            for (int u = 0; u < kHq; ++u) d[u] = dact[0][u];
+        }
+        // ---- stage A_bwd (delta1 scaled, hi | lo: this thread's k) and B_bwd
+        // in the A_fwd region
         __half* Bhi = (__half*)sA;
         __half* Ahi = (__half*)(sA + P.szBb);
         __half* Alo = (__half*)(sA + P.szBb + P.szAb / 2);
         const float sd = m.tc_sdelta;
 #pragma unroll
-        for (int k = 0; k < kH; ++k) {
+        for (int u = 0; u < kHq; ++u) {
             __half h, lo;
-            split_h(live ? d[k] * sd : 0.f, h, lo);
-            const uint32_t o2 = cm_off(row, k, kM) >> 1;
+            split_h(live ? d[u] * sd : 0.f, h, lo);
+            const uint32_t o2 = cm_off(row, o0 + u, kM) >> 1;
             Ahi[o2] = h;
             Alo[o2] = lo;
         }
@@ -418,9 +473,9 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
         if (ok) {
             const float inv = m.tc_inv_s1[e] / m.tc_sdelta;
             float* out = b.dEdGf + (size_t)atom * m.nsf_max;
-            for (int c0 = 0; c0 < P.nch * P.chN; c0 += 32) {
+            for (int c0 = 32 * quarter; c0 < P.nch * P.chN; c0 += 32 * kQ) {
                 float v[32];
-                tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kH + c0), v);
+                tmem_ld32(tbase + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(kH + c0), v);
                 if (live) {
                     if ((m.nsf_max & 3) == 0 && c0 + 32 <= nin) {
 #pragma unroll
