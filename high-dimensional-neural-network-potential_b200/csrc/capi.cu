@@ -446,8 +446,8 @@ int upload_model(hdnnp_model* m) {
         // b1, then each later layer's W and bias zero-padded to kH x kH and kH
         const size_t wsmall = kH + (size_t)(L - 1) * (kH * kH + kH);
         // (after GEMM 1 the A_fwd region holds B_bwd, A_bwd and the hidden
-        // layers' activation exchange, two 128 x kH FP32 buffers)
-        const size_t total = std::max(szA, szBb + szAb + (size_t)2 * 128 * kH * 4) + szBf +
+        // layers' activation exchange, two 128 x 36 FP32 buffers)
+        const size_t total = std::max(szA, szBb + szAb + (size_t)2 * 128 * 36 * 4) + szBf +
                              ((wsmall * 4 + 15) & ~size_t(15)) + 64;
         ok = ok && total <= 227 * 1024;
         if (ok) {

@@ -35,6 +35,8 @@ constexpr int kThr = 512;      // threads per CTA: 16 warps; warp w serves TMEM 
                                // 32 (w % 4) .. +31 and quarter w / 4 of each layer's neurons
 constexpr int kQ = kThr / kM;  // threads per row (4)
 constexpr int kHq = 32 / kQ;   // neurons of a padded layer per thread (8)
+constexpr int kX = 36;         // row stride (floats) of the activation exchange: 144 B rows,
+                               // float4 accesses of a warp free of bank conflicts
 constexpr int kH = 32;         // padded hidden width (N of GEMM 1, K of GEMM 2)
 constexpr int kTmemCols = 512;
 constexpr long long kWaitIters = 1LL << 22;
@@ -156,7 +158,7 @@ __host__ __device__ inline TCPlan tc_plan(const DevModel& m) {
     p.szW = ((w * 4) + 15) & ~size_t(15);
     // the A_fwd region after GEMM 1: B_bwd | A_bwd, then the activation
     // exchange of the hidden layers (two [kM][kH] FP32 buffers)
-    size_t reuse = p.szBb + p.szAb + (size_t)2 * kM * kH * 4;
+    size_t reuse = p.szBb + p.szAb + (size_t)2 * kM * kX * 4;
     p.total = (p.szA > reuse ? p.szA : reuse) + p.szBf + p.szW + 64;
     return p;
 }
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
     const int H = m.width[1];
     constexpr int L = NL;
     unsigned char* sA = sm;
-    const size_t reuse = P.szBb + P.szAb + (size_t)2 * kM * kH * 4;  // B_bwd | A_bwd | exchange
+    const size_t reuse = P.szBb + P.szAb + (size_t)2 * kM * kX * 4;  // B_bwd | A_bwd | exchange
     unsigned char* sBf = sm + (P.szA > reuse ? P.szA : reuse);
     float* sW = (float*)(sBf + P.szBf);
     uint64_t* mbar = (uint64_t*)((unsigned char*)sW + P.szW);
@@ -300,9 +302,9 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
 
     const bool live = row < cnt;
     const int atom = live ? b.el_atoms[t0 + row] : 0;
-    // activation exchange: two [kM][kH] buffers after B_bwd | A_bwd in the A_fwd region
+    // activation exchange: two [kM][kX] buffers after B_bwd | A_bwd in the A_fwd region
     float* xa = (float*)(sA + P.szBb + P.szAb);
-    float* xb = xa + kM * kH;
+    float* xb = xa + kM * kX;
     const int o0 = quarter * kHq;  // this thread's neurons o0 .. o0 + kHq - 1
     if (ok) {
         constexpr int kWB = kH * kH + kH;
@@ -312,21 +314,31 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
         tmem_ld32(tbase + ((uint32_t)((warp & 3) * 32) << 16), v);
         const float inv = m.tc_inv_s1[e];
         float dact[NL][kHq];  // act'(c) of this thread's neurons of every layer
+        // own eight values of a row of the exchange buffer, as two float4
+        auto put8 = [&](float* buf, const float (&x)[kHq]) {
+            float4* d4 = (float4*)(buf + row * kX + o0);
+            d4[0] = make_float4(x[0], x[1], x[2], x[3]);
+            d4[1] = make_float4(x[4], x[5], x[6], x[7]);
+        };
         // first hidden layer: own neurons, activations to the exchange buffer
+        {
+            float y8[kHq];
 #pragma unroll
-        for (int u = 0; u < kHq; ++u) {
-            const int o = o0 + u;
-            float c = 0.f, yv = 0.f, dv = 0.f;
+            for (int u = 0; u < kHq; ++u) {
+                const int o = o0 + u;
+                float c = 0.f, yv = 0.f, dv = 0.f;
 #pragma unroll
-            for (int qq = 0; qq < kQ; ++qq)  // v[o] with a compile-time index
-                if (qq == quarter) c = v[qq * kHq + u];
-            if (o < H) {
-                c = c * inv + sW[o];
-                yv = act_fw(m.act[0], c);
-                dv = act_dv(m.act[0], c, yv);
+                for (int qq = 0; qq < kQ; ++qq)  // v[o] with a compile-time index
+                    if (qq == quarter) c = v[qq * kHq + u];
+                if (o < H) {
+                    c = c * inv + sW[o];
+                    yv = act_fw(m.act[0], c);
+                    dv = act_dv(m.act[0], c, yv);
+                }
+                y8[u] = yv;
+                dact[0][u] = dv;
             }
-            xa[row * kH + o] = yv;
-            dact[0][u] = dv;
+            put8(xa, y8);
         }
         __syncthreads();
         // Layers 2..L: each thread its neurons from the whole previous layer
@@ -343,10 +355,10 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
             const float4* W4 = (const float4*)(sW + woff(l));
             const float* bb = sW + boff(l);
             const char al = m.act[l];
-            float yp[kH];
+            float yp[kH], y8[kHq];
 #pragma unroll
             for (int q = 0; q < kH / 4; ++q) {
-                const float4 t = *(const float4*)(cur + row * kH + 4 * q);
+                const float4 t = *(const float4*)(cur + row * kX + 4 * q);
                 yp[4 * q] = t.x; yp[4 * q + 1] = t.y; yp[4 * q + 2] = t.z; yp[4 * q + 3] = t.w;
             }
 #pragma unroll
@@ -366,10 +378,11 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
                     yv = act_fw(al, c);
                     dv = act_dv(al, c, yv);
                 }
-                nxt[row * kH + o] = yv;
+                y8[u] = yv;
                 dact[l][u] = dv;
                 if (l == NL - 1 && o == 0) yout = yv;
             }
+            put8(nxt, y8);
             __syncthreads();
             float* t = cur;
             cur = nxt;
@@ -379,8 +392,7 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
         // backward (gradOut = 1) down to the first hidden layer: deltas of
         // this thread's neurons; the whole delta vector of a layer through
         // the exchange buffer
-#pragma unroll
-        for (int u = 0; u < kHq; ++u) cur[row * kH + o0 + u] = dact[NL - 1][u];
+        put8(cur, dact[NL - 1]);
         __syncthreads();
         float d[kHq];
 #pragma unroll
@@ -390,7 +402,7 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
             float dl[kH];
 #pragma unroll
             for (int q = 0; q < kH / 4; ++q) {
-                const float4 t = *(const float4*)(cur + row * kH + 4 * q);
+                const float4 t = *(const float4*)(cur + row * kX + 4 * q);
                 dl[4 * q] = t.x; dl[4 * q + 1] = t.y; dl[4 * q + 2] = t.z; dl[4 * q + 3] = t.w;
             }
             float g[kHq];
@@ -413,8 +425,7 @@ __global__ void __launch_bounds__(kThr, 1) k_mlp_tc(Batch b, DevModel m) {
 #pragma unroll
             for (int u = 0; u < kHq; ++u) d[u] = g[u] * dact[l - 1][u];
             if (l > 1) {
-#pragma unroll
-                for (int u = 0; u < kHq; ++u) nxt[row * kH + o0 + u] = d[u];
+                put8(nxt, d);
                 __syncthreads();
                 float* t = cur;
                 cur = nxt;
