@@ -195,6 +195,7 @@ struct hdnnp_ctx {
     DevBuf<double> cm_acc, cm_E, cm_std;                  // committee: dE/dG sum, member energies, std
     DevBuf<unsigned> pairs;                               // contributing-pair lists (fast kernels)
     DevBuf<int> npairs;
+    DevBuf<int> cnei_cnt, cnei_off, cnei_j, cnei_s, cnei_rev, cnei_map;  // compacted Verlet-skin lists
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -219,6 +220,7 @@ struct hdnnp_ctx {
         stats.release();
         pairs.release();
         npairs.release();
+        for (auto* b : {&cnei_cnt, &cnei_off, &cnei_j, &cnei_s, &cnei_rev, &cnei_map}) b->release();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
@@ -682,6 +684,12 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.nei_s = c->nei_s.p;
     b.nei_rev = c->nei_rev.p;
     b.gent = c->gent.p;
+    // Verlet-skin lists: the stages after the list read a compacted copy
+    const bool compact = b.rc_list > D.max_rc;
+    if (compact && ((r = c->cnei_cnt.ensure(N + 1)) || (r = c->cnei_off.ensure(N + 1)) ||
+                    (r = c->cnei_j.ensure(E + 1)) || (r = c->cnei_s.ensure(E + 1)) ||
+                    (r = c->cnei_rev.ensure(E + 1)) || (r = c->cnei_map.ensure(E + 1))))
+        return r;
     // mixed precision runs on the fast (lambda x zeta x eta) kernels; potentials
     // outside their shapes evaluate in FP64 with the generic kernels
     const bool fast = D.fast && !c->generic_sf;
@@ -721,6 +729,16 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     }
     if ((r = mark(1))) return r;  // after the host read: stage 1 starts here
     L += launch_neighbour_build_b(b, D, st);
+    if (compact) {
+        const CompactLists cl{c->cnei_cnt.p, c->cnei_off.p, c->cnei_j.p, c->cnei_s.p, c->cnei_rev.p, c->cnei_map.p};
+        L += launch_compact_lists(b, D.max_rc, cl, st);
+        b.nei_cnt = cl.cnt;
+        b.nei_off = cl.off;
+        b.nei_j = cl.nj;
+        b.nei_s = cl.ns;
+        b.nei_rev = cl.rev;
+        b.rc_list = D.max_rc;  // entries beyond an element's own cutoff are still dropped
+    }
     if ((r = mark(2))) return r;
     L += launch_element_groups(b, D, st);
     if ((r = mark(3))) return r;

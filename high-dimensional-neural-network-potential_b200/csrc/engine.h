@@ -155,8 +155,10 @@ struct Batch {
     float* gselff;
     float* virf;
     // Resident plans (plan.cu).  rc_list: neighbour-list cutoff (0: the
-    // potential's max_rc; max_rc + skin for Verlet-skin lists, whose entries
-    // beyond rc the symmetry-function kernels drop).  rebuild: device flag,
+    // potential's max_rc; max_rc + skin for Verlet-skin lists, which the
+    // stages after the list read compacted to max_rc, with rc_list = max_rc;
+    // the symmetry-function kernels drop entries beyond an element's own rc
+    // when rc_list is above it).  rebuild: device flag,
     // null = build every evaluation; when it is 0 the list, cells and wrap
     // translations of the last build are kept and positions are translated
     // by wshift instead of wrapped.  wshift[3*natoms]: wrapped - raw position
@@ -204,6 +206,14 @@ struct PipePlan {
 struct CtxLists {
     int *elem, *cnt, *off, *nj, *ns, *rev;
 };
+
+// Compacted copy of a Verlet-skin list (launch_compact_lists in
+// neighbors.cu): cnt/off [natoms+1], nj/ns/rev [entries], map [entries of
+// the full list] (compacted index or -1).
+struct CompactLists {
+    int *cnt, *off, *nj, *ns, *rev, *map;
+};
+int launch_compact_lists(const Batch& b, double rc, const CompactLists& c, cudaStream_t s);
 
 // Committee of potentials (committee.cu; globalHdnnpEnergyAndForces,
 // globalHdnnps.f90:31-70): neighbour lists and symmetry functions of the

@@ -463,6 +463,90 @@ int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) 
     return 2;
 }
 
+// ---------------------------------------------------------------- skin lists
+// A Verlet-skin list (cutoff max_rc + skin) holds about (1 + skin/rc)^3 times
+// the entries that contribute.  Every evaluation copies the entries closer
+// than max_rc into a second CSR list, in list order, and remaps the reverse
+// index onto it; the symmetry-function and force stages then read only that
+// list.  The test computes d = (x_a - x_j) - L(S) in FP64 with every step
+// negated exactly for the reverse entry (x_j - x_a) - L(-S) (round to nearest
+// is symmetric), so an entry and its reverse are kept or dropped together.
+namespace {
+
+__device__ __forceinline__ bool entry_inside(const Batch& b, const StructInfo& S, double xa, double ya, double za,
+                                             int j, int sh, double rc2) {
+    int sx, sy, sz;
+    unpack_shift(sh, sx, sy, sz);
+    const double* h = S.h;
+    double lx = 0, ly = 0, lz = 0;
+    if (sz) { lx += h[6] * sz; ly += h[7] * sz; lz += h[8] * sz; }
+    if (sy) { lx += h[3] * sy; ly += h[4] * sy; lz += h[5] * sy; }
+    if (sx) { lx += h[0] * sx; ly += h[1] * sx; lz += h[2] * sx; }
+    const double dx = (xa - b.wpos[3 * j]) - lx, dy = (ya - b.wpos[3 * j + 1]) - ly, dz = (za - b.wpos[3 * j + 2]) - lz;
+    return dx * dx + dy * dy + dz * dz < rc2;
+}
+
+// One warp per atom: kFill = false counts the kept entries (ccnt, and coff
+// for the scan); kFill = true writes them at coff and maps every entry of
+// the full list to its compacted index (-1: dropped).
+template <bool kFill>
+__global__ void k_compact(Batch b, double rc2, int* ccnt, int* coff, int* cj, int* cs, int* cmap) {
+    const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= b.natoms) return;  // uniform per warp
+    const int e0 = b.nei_off[a], e1 = b.nei_off[a + 1];
+    const StructInfo& S = b.info[b.sid[a]];
+    const double xa = b.wpos[3 * a], ya = b.wpos[3 * a + 1], za = b.wpos[3 * a + 2];
+    int n = kFill ? coff[a] : 0;
+    for (int base = e0; base < e1; base += 32) {
+        const int e = base + lane;
+        int j = 0, sh = 0;
+        bool in = false;
+        if (e < e1) {
+            j = b.nei_j[e];
+            sh = b.nei_s[e];
+            in = entry_inside(b, S, xa, ya, za, j, sh, rc2);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (kFill && e < e1) {
+            const int o = n + __popc(m & ((1u << lane) - 1u));
+            if (in) {
+                cj[o] = j;
+                cs[o] = sh;
+            }
+            cmap[e] = in ? o : -1;
+        }
+        n += __popc(m);
+    }
+    if (!kFill && lane == 0) {
+        ccnt[a] = n;
+        coff[a] = n;
+    }
+}
+
+// Reverse index of the compacted list, one thread per entry of the full list.
+__global__ void k_compact_rev(Batch b, const int* cmap, int* crev) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= b.nei_off[b.natoms]) return;
+    const int o = cmap[e];
+    if (o < 0) return;
+    const int r = cmap[b.nei_rev[e]];
+    if (r < 0) atomicOr(&b.status[0], 2);  // asymmetric list (should not happen)
+    crev[o] = r < 0 ? o : r;
+}
+
+}  // namespace
+
+int launch_compact_lists(const Batch& b, double rc, const CompactLists& c, cudaStream_t s) {
+    const unsigned gW = (unsigned)((32LL * b.natoms + kThreads - 1) / kThreads);
+    const double rc2 = rc * rc;
+    k_compact<false><<<gW, kThreads, 0, s>>>(b, rc2, c.cnt, c.off, nullptr, nullptr, nullptr);
+    int L = 1 + launch_scan(c.off, b.natoms, b.scan_tmp, nullptr, s);
+    k_compact<true><<<gW, kThreads, 0, s>>>(b, rc2, c.cnt, c.off, c.nj, c.ns, c.map);
+    k_compact_rev<<<(unsigned)(((long long)b.nentries + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, c.map, c.rev);
+    return L + 2;
+}
+
 // ---------------------------------------------------------------- planned capacities
 namespace {
 

@@ -12,8 +12,8 @@
 // Molecules get their bounding box on the device.  With a skin, lists are
 // built with cutoff rc + skin and kept until an atom has moved more than
 // skin / 2 since the last build (checked on the device each evaluation);
-// entries beyond rc contribute nothing and are dropped by the
-// symmetry-function kernels.  Overflow of the planned capacities is flagged
+// every evaluation copies the entries within rc into a compacted list that
+// the later stages read (launch_compact_lists).  Overflow of the planned capacities is flagged
 // on the device (no access leaves the reserved arrays) and reported by
 // hdnnp_plan_sync as HDNNP_E_CAPACITY; the plan must then be recreated.
 #include <cuda_runtime.h>

@@ -179,6 +179,36 @@ def test_skin_lists_match_rebuilt_lists(pot, PL, W, precision):
             assert np.abs(ea - eb).max() / len(s["Z"]) <= 1e-6
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_skin_lists_are_compacted(pot, PL, W, precision):
+    """The stages after the list read only the entries of a skin list that lie
+    within rc: as many as a list built without the skin, in a cell whose atoms
+    moved after the build (kept list), for a batch of cells and a molecule."""
+    import torch
+
+    structs = cells(W, [(3, 3, 3), (2, 2, 1)], 21)
+    mol = W.abx3_cell()
+    structs.append({"Z": mol["Z"], "pos": mol["pos"] + 1.0, "lat": None})
+    kw = dict(precision=precision, profile=True)
+    with PL.Plan(pot, structs, skin=0.0, **kw) as a, PL.Plan(pot, structs, skin=1.0, **kw) as b:
+        rng = np.random.default_rng(4)
+        step = torch.from_numpy(rng.normal(0.0, 0.08, tuple(a.pos.shape))).to(a.pos.device)
+        for q in (a, b):
+            q.launch()
+            q.sync()
+            q.pos.add_(step)  # |step| < skin/2 for every atom: b keeps its list
+            q.profile(reset=True)
+            q.launch()
+        assert a.sync() == 1 and b.sync() == 0
+        ca, cb = a.profile()[1], b.profile()[1]
+        assert cb["entries"] == ca["entries"] and cb["pairs"] == ca["pairs"]
+        Ea, Fa, _ = a.results()
+        Eb, Fb, _ = b.results()
+        tol_e, tol_f = (1e-10, 1e-9) if precision == 0 else (1e-6, 1e-5)
+        assert np.abs(Ea - Eb).max() <= tol_e * np.abs(Ea).max()
+        assert np.abs(Fa - Fb).max() <= tol_f
+
+
 def test_capacity_overflow_is_flagged(pot, PL, W):
     import torch
     from hdnnp_b200.engine import HdnnpError
