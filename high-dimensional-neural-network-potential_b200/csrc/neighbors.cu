@@ -11,8 +11,10 @@
 // The atom itself is not stored (the reference keeps it as entry 1); the
 // symmetry-function kernels treat it implicitly.
 //
-// HBM-bound integer/FP64 work: one thread per atom (wrap, count, fill, force
-// gather), one warp per atom (reverse index), one thread per cell (sort).
+// HBM-bound integer/FP64 work: a thread per atom (wrap), a thread or a warp
+// per atom (count, fill), one or more warps per atom (reverse index), a warp
+// per cell (sort) and per atom (skin-list compaction).
+#include <algorithm>
 #include <cmath>
 
 #include "engine.h"
@@ -318,17 +320,20 @@ inline bool warp_lists(const Batch& b) {
 }
 
 // Reverse-entry index: for entry e = (a -> j, shift s) the entry (j -> a, -s)
-// of j's list.  One warp per atom a; for each of a's entries the 32 lanes scan
-// j's list in coalesced 32-entry chunks and the ballot picks the first match.
-__global__ void k_reverse(Batch b) {
-    const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+// of j's list.  `parts` warps per atom a, each taking every parts-th group
+// of four entries; one search per group of 8 lanes, which scan j's list in
+// coalesced 8-entry chunks, the ballot picking the first match.  Small
+// batches use several warps per atom so that enough searches are in flight.
+__global__ void k_reverse(Batch b, int parts) {
+    const long long w = (long long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int a = (int)(w / parts), part = (int)(w % parts);
     const int lane = threadIdx.x & 31;
     if (a >= b.natoms || keep_list(b)) return;  // uniform per warp
     // four entries of atom a at a time, one per group of 8 lanes, so that the
     // dependent loads of four searches overlap
     const int grp = lane >> 3, gl = lane & 7;
     const int e1 = b.nei_off[a + 1];
-    for (int e0 = b.nei_off[a]; e0 < e1; e0 += 4) {
+    for (int e0 = b.nei_off[a] + 4 * part; e0 < e1; e0 += 4 * parts) {
         const int e = e0 + grp;
         const bool live = e < e1;
         int want = 0, f0 = 0, f1 = 0;
@@ -459,7 +464,9 @@ int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) 
         k_neighbours_warp<true><<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
     else
         k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
-    k_reverse<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
+    // warps per atom: up to 8, until ~64 warps per SM of a B200 are in flight
+    const int parts = (int)std::min<long long>(8, std::max<long long>(1, (148LL * 64 + b.natoms - 1) / std::max(b.natoms, 1)));
+    k_reverse<<<(unsigned)((warps_threads * parts + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, parts);
     return 2;
 }
 

@@ -17,21 +17,34 @@ namespace hdnnp {
 
 namespace {
 
+// One warp per atom: lane l sums the reverse-entry gradients of entries
+// e0 + l, e0 + l + 32, ... in order (coalesced index loads), a butterfly
+// combines the lanes and lane 0 adds g_self.  The order depends only on the
+// atom's own list, so a structure gets the same forces alone and in a batch.
 template <typename T>
 __global__ void k_force_gather(Batch b, const T* gself, const T* gent) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= b.natoms) return;
-    double fx = gself[3 * (size_t)a], fy = gself[3 * (size_t)a + 1], fz = gself[3 * (size_t)a + 2];
+    const int a = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= b.natoms) return;  // uniform per warp
+    double fx = 0.0, fy = 0.0, fz = 0.0;
     const int e0 = b.nei_off[a], e1 = b.nei_off[a + 1];
-    for (int e = e0; e < e1; ++e) {
+    for (int e = e0 + lane; e < e1; e += 32) {
         const size_t r = (size_t)b.nei_rev[e];
         fx += gent[3 * r];
         fy += gent[3 * r + 1];
         fz += gent[3 * r + 2];
     }
-    b.force[3 * (size_t)a] = -fx;
-    b.force[3 * (size_t)a + 1] = -fy;
-    b.force[3 * (size_t)a + 2] = -fz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (lane == 0) {
+        b.force[3 * (size_t)a] = -((double)gself[3 * (size_t)a] + fx);
+        b.force[3 * (size_t)a + 1] = -((double)gself[3 * (size_t)a + 1] + fy);
+        b.force[3 * (size_t)a + 2] = -((double)gself[3 * (size_t)a + 2] + fz);
+    }
 }
 
 // Neumaier running sum
@@ -139,7 +152,7 @@ int launch_struct_energies(const Batch& b, bool fp32, double* out, cudaStream_t 
 
 int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s) {
     (void)m;
-    k_force_gather<double><<<(b.natoms + 255) / 256, 256, 0, s>>>(b, b.gself, b.gent);
+    k_force_gather<double><<<(unsigned)((32LL * b.natoms + 255) / 256), 256, 0, s>>>(b, b.gself, b.gent);
     k_struct_reduce<double><<<b.nstruct, kRedThreads, 0, s>>>(b, want_dEdLat, b.atE, b.vir);
     return 2;
 }
@@ -147,7 +160,7 @@ int launch_forces_and_reduce(const Batch& b, const DevModel& m, int want_dEdLat,
 // mixed-precision form: FP32 intermediates, FP64 accumulation and outputs
 int launch_forces_and_reduce_fp32(const Batch& b, const DevModel& m, int want_dEdLat, cudaStream_t s) {
     (void)m;
-    k_force_gather<float><<<(b.natoms + 255) / 256, 256, 0, s>>>(b, b.gselff, b.gentf);
+    k_force_gather<float><<<(unsigned)((32LL * b.natoms + 255) / 256), 256, 0, s>>>(b, b.gselff, b.gentf);
     k_struct_reduce<float><<<b.nstruct, kRedThreads, 0, s>>>(b, want_dEdLat, b.atEf, b.virf);
     return 2;
 }
