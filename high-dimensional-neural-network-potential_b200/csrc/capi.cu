@@ -647,7 +647,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
     if ((r = mark(0))) return r;
     if (pp && pp->dev_boxes) L += launch_molecule_boxes(b, pp->rc_list > 0.0 ? pp->rc_list : D.max_rc, st);
-    L += launch_neighbour_build_a(b, D, st);
+    L += launch_neighbour_build_a(b, D, st, pp && !pp->upload);
     size_t E = 0;
     if (pp && pp->e_cap > 0) {
         // planned: no host read; overflow of the capacities is flagged on the device

@@ -253,8 +253,11 @@ __host__ __device__ inline void unpack_shift(int p, int& x, int& y, int& z) {
 
 // ------------------------------------------------------------------ launchers
 // Each returns the number of kernel launches it issued.
-int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s);  // wrap, bin, count
+// wrap, bin, count; sid_valid: the atom -> structure map of an earlier
+// evaluation of the same batch is still in place (plan replays)
+int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, bool sid_valid = false);
 int launch_scan(int* data, int n, int* tmp, int* total_out_dev, cudaStream_t s);   // exclusive scan in place, total in data[n]
+int launch_scan_from(const int* src, int* data, int n, int* tmp, cudaStream_t s);  // the same from src (src may be data)
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s);  // fill + reverse
 // Planned evaluations (no host read between the count and the fill pass):
 // flag 32 and empty lists when the entries or the largest count exceed the

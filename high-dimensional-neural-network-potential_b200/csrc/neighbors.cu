@@ -373,12 +373,13 @@ __global__ void k_max_count(const int* cnt, int n, int* out) {
 // ---------------------------------------------------------------- scan
 // Exclusive scan of n ints in place (data[n] receives the total).  Two-level:
 // per-block scan of 1024 values, scan of block sums (recursive), add.
-__global__ void k_scan_block(int* d, int n, int* sums) {
+// src may equal d (in place); a single block also writes the total to d[n].
+__global__ void k_scan_block(const int* src, int* d, int n, int* sums) {
     __shared__ int wsum[32];
     int base = blockIdx.x * 1024;
     int t = threadIdx.x;  // 1024 threads
     int i = base + t;
-    int v = i < n ? d[i] : 0;
+    int v = i < n ? src[i] : 0;
     int lane = t & 31, w = t >> 5;
     int x = v;
     for (int o = 1; o < 32; o <<= 1) {
@@ -398,46 +399,52 @@ __global__ void k_scan_block(int* d, int n, int* sums) {
     __syncthreads();
     int incl = x + (w > 0 ? wsum[w - 1] : 0);
     if (i < n) d[i] = incl - v;
-    if (t == 1023) sums[blockIdx.x] = incl;
+    if (t == 1023) {
+        sums[blockIdx.x] = incl;
+        if (gridDim.x == 1) d[n] = incl;
+    }
 }
 
+// sums[gridDim.x] holds the grand total (the recursive scan of the block sums)
 __global__ void k_scan_add(int* d, int n, const int* sums) {
     int i = blockIdx.x * 1024 + threadIdx.x;
     if (i < n && blockIdx.x > 0) d[i] += sums[blockIdx.x];
+    if (blockIdx.x == 0 && threadIdx.x == 0) d[n] = sums[gridDim.x];
 }
 
 }  // namespace
 
-int launch_scan(int* data, int n, int* tmp, int* total_unused, cudaStream_t s) {
-    (void)total_unused;
+int launch_scan_from(const int* src, int* data, int n, int* tmp, cudaStream_t s) {
     int launches = 0;
     int nb = (n + 1023) / 1024;
     if (nb <= 0) nb = 1;
     // tmp must hold nb + 1 ints, plus space for the recursion
-    k_scan_block<<<nb, 1024, 0, s>>>(data, n, tmp);
+    k_scan_block<<<nb, 1024, 0, s>>>(src, data, n, tmp);
     ++launches;
     if (nb > 1) {
         launches += launch_scan(tmp, nb, tmp + nb + 1, nullptr, s);  // tmp[nb] = grand total
-        k_scan_add<<<nb, 1024, 0, s>>>(data, n, tmp);
+        k_scan_add<<<nb, 1024, 0, s>>>(data, n, tmp);                // also data[n] = total
         ++launches;
-        // data[n] = total
-        cudaMemcpyAsync(data + n, tmp + nb, sizeof(int), cudaMemcpyDeviceToDevice, s);
-    } else {
-        cudaMemcpyAsync(data + n, tmp, sizeof(int), cudaMemcpyDeviceToDevice, s);
     }
     return launches;
 }
 
-int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s) {
+int launch_scan(int* data, int n, int* tmp, int* total_unused, cudaStream_t s) {
+    (void)total_unused;
+    return launch_scan_from(data, data, n, tmp, s);
+}
+
+int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, bool sid_valid) {
     int L = 0;
     const int gA = (b.natoms + kThreads - 1) / kThreads;
-    k_atom_struct<<<b.nstruct, 128, 0, s>>>(b.info, b.nstruct, b.sid);
-    ++L;
+    if (!sid_valid) {
+        k_atom_struct<<<b.nstruct, 128, 0, s>>>(b.info, b.nstruct, b.sid);
+        ++L;
+    }
     cudaMemsetAsync(b.cell_cnt, 0, sizeof(int) * (b.ncells + 1), s);
     k_wrap_bin<<<gA, kThreads, 0, s>>>(b, m);
     ++L;
-    cudaMemcpyAsync(b.cell_start, b.cell_cnt, sizeof(int) * (b.ncells + 1), cudaMemcpyDeviceToDevice, s);
-    L += launch_scan(b.cell_start, b.ncells, b.scan_tmp, nullptr, s);
+    L += launch_scan_from(b.cell_cnt, b.cell_start, b.ncells, b.scan_tmp, s);
     cudaMemsetAsync(b.cell_cnt, 0, sizeof(int) * (b.ncells + 1), s);
     k_fill_cells<<<gA, kThreads, 0, s>>>(b, b.cell_cnt);
     ++L;
@@ -448,8 +455,7 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s) 
     else
         k_neighbours<false><<<gA, kThreads, 0, s>>>(b, m);
     ++L;
-    cudaMemcpyAsync(b.nei_off, b.nei_cnt, sizeof(int) * b.natoms, cudaMemcpyDeviceToDevice, s);
-    L += launch_scan(b.nei_off, b.natoms, b.scan_tmp, nullptr, s);
+    L += launch_scan_from(b.nei_cnt, b.nei_off, b.natoms, b.scan_tmp, s);
     // status[1] = max count
     cudaMemsetAsync(b.status + 1, 0, sizeof(int), s);
     k_max_count<<<gA, kThreads, 0, s>>>(b.nei_cnt, b.natoms, b.status + 1);

@@ -19,6 +19,8 @@
 // one exp per distinct eta.  Warp per centre atom; neighbours staged in
 // shared memory sorted by element; candidate pairs compacted through a shared
 // queue; chunks of 32 contributing pairs, one per lane.
+#include <algorithm>
+
 #include "engine.h"
 
 namespace hdnnp {
@@ -851,8 +853,15 @@ constexpr int kBlocksPerSm = 32;
 template <typename T, class S>
 int run_spec(const Batch& b, const DevModel& m, bool grad, cudaStream_t st) {
     const int mfull = b.mmax > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
-    const int split = b.sf_split > 0 ? b.sf_split : b.sf_split < 0 ? mfull : kSplitCount;
+    int split = b.sf_split > 0 ? b.sf_split : b.sf_split < 0 ? mfull : kSplitCount;
     const int per_sm = b.sf_blocks_per_sm > 0 ? b.sf_blocks_per_sm : kBlocksPerSm;
+    if (b.sf_split == 0 && mfull > split) {
+        // a batch whose warps all fit on the GPU at the full size needs no
+        // second launch (same code per atom: same results)
+        const size_t blk = fast_warp_bytes<T>(mfull, m.g2max, m.nblk, S::P, grad) * kWarps;
+        const int fit = std::min<int>(sizeof(T) == 4 ? (grad ? 8 : 7) : 4, (int)((227u * 1024u) / blk));
+        if ((long long)b.natoms <= (long long)nsm() * fit * kWarps) split = mfull;
+    }
     int L = 0;
     auto go = [&](int mm, int mlo, int last) {
         const size_t smem = fast_warp_bytes<T>(mm, m.g2max, m.nblk, S::P, grad) * kWarps;
