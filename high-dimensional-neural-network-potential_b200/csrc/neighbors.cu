@@ -324,9 +324,11 @@ inline bool warp_lists(const Batch& b) {
 // of four entries; one search per group of 8 lanes, which scan j's list in
 // coalesced 8-entry chunks, the ballot picking the first match.  Small
 // batches use several warps per atom so that enough searches are in flight.
+template <bool kMulti>
 __global__ void k_reverse(Batch b, int parts) {
     const long long w = (long long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
-    const int a = (int)(w / parts), part = (int)(w % parts);
+    if (!kMulti) parts = 1;
+    const int a = kMulti ? (int)(w / parts) : (int)w, part = kMulti ? (int)(w % parts) : 0;
     const int lane = threadIdx.x & 31;
     if (a >= b.natoms || keep_list(b)) return;  // uniform per warp
     // four entries of atom a at a time, one per group of 8 lanes, so that the
@@ -472,7 +474,11 @@ int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) 
         k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
     // warps per atom: up to 8, until ~64 warps per SM of a B200 are in flight
     const int parts = (int)std::min<long long>(8, std::max<long long>(1, (148LL * 64 + b.natoms - 1) / std::max(b.natoms, 1)));
-    k_reverse<<<(unsigned)((warps_threads * parts + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, parts);
+    const unsigned gR = (unsigned)((warps_threads * parts + kThreads - 1) / kThreads);
+    if (parts > 1)
+        k_reverse<true><<<gR, kThreads, 0, s>>>(b, parts);
+    else
+        k_reverse<false><<<gR, kThreads, 0, s>>>(b, 1);
     return 2;
 }
 
