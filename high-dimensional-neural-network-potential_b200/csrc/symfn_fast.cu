@@ -128,7 +128,9 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 __device__ __forceinline__ double xsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double xexp(double x) { return exp(x); }
-__device__ __forceinline__ float xexp(float x) { return expf(x); }
+// FP32 form: the exp2-based intrinsic (max error 2 + floor(1.173 |x|) ulp;
+// the angular arguments stay below ~5, where it is within 8 ulp)
+__device__ __forceinline__ float xexp(float x) { return __expf(x); }
 __device__ __forceinline__ double xtanh(double x) { return tanh(x); }
 __device__ __forceinline__ float xtanh(float x) { return tanhf(x); }
 __device__ __forceinline__ double xpow(double x, double y) { return pow(x, y); }
