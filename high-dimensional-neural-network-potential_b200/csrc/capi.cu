@@ -196,6 +196,7 @@ struct hdnnp_ctx {
     DevBuf<unsigned> pairs;                               // contributing-pair lists (fast kernels)
     DevBuf<int> npairs;
     DevBuf<int> cnei_cnt, cnei_off, cnei_j, cnei_s, cnei_rev, cnei_map;  // compacted Verlet-skin lists
+    DevBuf<int> pad;                                      // padded neighbour rows of plans (int2 pairs)
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -220,7 +221,7 @@ struct hdnnp_ctx {
         stats.release();
         pairs.release();
         npairs.release();
-        for (auto* b : {&cnei_cnt, &cnei_off, &cnei_j, &cnei_s, &cnei_rev, &cnei_map}) b->release();
+        for (auto* b : {&cnei_cnt, &cnei_off, &cnei_j, &cnei_s, &cnei_rev, &cnei_map, &pad}) b->release();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
@@ -646,6 +647,12 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     };
     CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
     if ((r = mark(0))) return r;
+    if (pp && pp->pad_lists && pp->e_cap > 0) {
+        // capacities known: one search pass into padded rows (buffer sized by the probe)
+        if ((r = c->pad.ensure(2 * N * (size_t)pp->m_cap))) return r;
+        b.pad = reinterpret_cast<int2*>(c->pad.p);
+        b.pad_cap = pp->m_cap;
+    }
     if (pp && pp->dev_boxes) L += launch_molecule_boxes(b, pp->rc_list > 0.0 ? pp->rc_list : D.max_rc, st);
     L += launch_neighbour_build_a(b, D, st, pp && !pp->upload);
     size_t E = 0;
@@ -674,6 +681,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             pp->m_cap = (((int)std::ceil(b.mmax * f) + 8) + 31) / 32 * 32;
             E = (size_t)pp->e_cap;
             b.mmax = pp->m_cap;
+            if (pp->pad_lists && (r = c->pad.ensure(2 * N * (size_t)pp->m_cap))) return r;
         }
     }
     if ((r = c->nei_j.ensure(E + 1)) || (r = c->nei_s.ensure(E + 1)) || (r = c->nei_rev.ensure(E + 1)) ||

@@ -181,6 +181,11 @@ struct Batch {
     int sf_split;
     int sf_blocks_per_sm;
     int nei_warp;             // neighbour lists: 1 warp per atom, -1 thread per atom, 0 by batch size
+    // Plans: the neighbour search writes each atom's entries (j, packed
+    // shift) into a padded row of pad_cap in one pass, copied into the CSR
+    // arrays after the scan (pad_cap = 0: count pass, then fill pass).
+    int2* pad;                // [natoms * pad_cap]
+    int pad_cap;
 };
 
 constexpr int kPairCap = 1024;  // listed pairs per atom (the dense workloads average ~550)
@@ -200,6 +205,7 @@ struct PipePlan {
     int* rebuild = nullptr;  // Verlet-skin flag (null: rebuild every time)
     double* wshift = nullptr;
     double* pos_ref = nullptr;
+    bool pad_lists = false;  // one search pass into padded rows of m_cap (after the probe)
 };
 
 // Device neighbour-list arrays of a context (ctx_list_arrays in capi.cu).

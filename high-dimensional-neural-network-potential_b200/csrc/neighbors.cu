@@ -147,12 +147,16 @@ __global__ void k_sort_cells(Batch b) {
 // floor of the exact quotient)
 __device__ __forceinline__ int floor_div(int a, int n) { return a >= 0 ? a / n : -((n - 1 - a) / n); }
 
-// K3 enumeration shared by the count and the fill pass.
-template <bool kFill>
+// K3 enumeration shared by the passes.  kMode 0: count; 1: fill the CSR
+// lists at nei_off; 2 (plans): count and fill the atom's padded row of
+// pad_cap entries in one pass (entries beyond pad_cap are counted only; the
+// capacity check then empties the lists), copied into the CSR arrays by
+// k_rows_to_lists after the scan.
+template <int kMode>
 __global__ void k_neighbours(Batch b, DevModel m) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= b.natoms || keep_list(b)) return;
-    if (kFill && b.status[3]) return;  // planned capacity exceeded: the lists stay empty
+    if (kMode == 1 && b.status[3]) return;  // planned capacity exceeded: the lists stay empty
     const StructInfo& S = b.info[b.sid[i]];
     const double rc = b.rc_list > 0.0 ? b.rc_list : m.max_rc, rc2 = rc * rc;
     const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
@@ -162,7 +166,8 @@ __global__ void k_neighbours(Batch b, DevModel m) {
     const int iz = c % S.ngrid[2];
     const double* h = S.h;
     int n = 0;
-    int out = kFill ? b.nei_off[i] : 0;
+    int out = kMode == 1 ? b.nei_off[i] : 0;
+    int2* row = kMode == 2 ? b.pad + (size_t)i * b.pad_cap : nullptr;
     for (int jx = -S.nsearch[0]; jx <= S.nsearch[0]; ++jx) {
         for (int jy = -S.nsearch[1]; jy <= S.nsearch[1]; ++jy) {
             for (int jz = -S.nsearch[2]; jz <= S.nsearch[2]; ++jz) {
@@ -197,11 +202,12 @@ __global__ void k_neighbours(Batch b, DevModel m) {
                     double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
                     double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
                     if (ddx * ddx + ddy * ddy + ddz * ddz < rc2) {
-                        if (kFill) {
+                        if (kMode == 1) {
                             b.nei_j[out] = j;
                             b.nei_s[out] = pack_shift(dx, dy, dz);
                             ++out;
                         } else {
+                            if (kMode == 2 && n < b.pad_cap) row[n] = make_int2(j, pack_shift(dx, dy, dz));
                             ++n;
                         }
                     }
@@ -209,7 +215,7 @@ __global__ void k_neighbours(Batch b, DevModel m) {
             }
         }
     }
-    if (!kFill) b.nei_cnt[i] = n;
+    if (kMode != 1) b.nei_cnt[i] = n;
 }
 
 // The same enumeration with one warp per atom: the virtual cells, in the
@@ -219,12 +225,12 @@ __global__ void k_neighbours(Batch b, DevModel m) {
 // list is the same, entry for entry.  For batches too small to fill the GPU
 // with a thread per atom (a single cell of a few hundred atoms has thousands
 // of candidates per atom, walked serially by one thread).
-template <bool kFill>
+template <int kMode>
 __global__ void k_neighbours_warp(Batch b, DevModel m) {
     const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= b.natoms || keep_list(b)) return;  // uniform per warp
-    if (kFill && b.status[3]) return;
+    if (kMode == 1 && b.status[3]) return;
     const StructInfo& S = b.info[b.sid[i]];
     const double rc = b.rc_list > 0.0 ? b.rc_list : m.max_rc, rc2 = rc * rc;
     const double xi = b.wpos[3 * i], yi = b.wpos[3 * i + 1], zi = b.wpos[3 * i + 2];
@@ -236,7 +242,8 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
     const int ny = 2 * S.nsearch[1] + 1, nz = 2 * S.nsearch[2] + 1;
     const int nv = (2 * S.nsearch[0] + 1) * ny * nz;
     int n = 0;
-    int out = kFill ? b.nei_off[i] : 0;
+    int out = kMode == 1 ? b.nei_off[i] : 0;
+    int2* row = kMode == 2 ? b.pad + (size_t)i * b.pad_cap : nullptr;
     for (int v0 = 0; v0 < nv; v0 += 32) {
         const int v = v0 + lane;
         int p0 = 0, p1 = 0, dx = 0, dy = 0, dz = 0;
@@ -289,8 +296,8 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
             if (lane >= d) incl += o;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (kFill && cnt > 0) {
-            int o = out + incl - cnt;
+        if (kMode != 0 && cnt > 0) {
+            int o = (kMode == 1 ? out : n) + incl - cnt;
             const int sh = pack_shift(dx, dy, dz);
             for (int p = p0; p < p1; ++p) {
                 const int j = b.cell_atoms[p];
@@ -298,8 +305,12 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
                 double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
                 double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
                 if (ddx * ddx + ddy * ddy + ddz * ddz < rc2) {
-                    b.nei_j[o] = j;
-                    b.nei_s[o] = sh;
+                    if (kMode == 1) {
+                        b.nei_j[o] = j;
+                        b.nei_s[o] = sh;
+                    } else if (o < b.pad_cap) {
+                        row[o] = make_int2(j, sh);
+                    }
                     ++o;
                 }
             }
@@ -307,7 +318,22 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
         out += total;
         n += total;
     }
-    if (!kFill && lane == 0) b.nei_cnt[i] = n;
+    if (kMode != 1 && lane == 0) b.nei_cnt[i] = n;
+}
+
+// Padded rows -> CSR lists (plans), one warp per atom.  After an overflow the
+// capacity check has emptied the lists (nei_off all 0), so nothing is copied.
+__global__ void k_rows_to_lists(Batch b) {
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= b.natoms || keep_list(b)) return;  // uniform per warp
+    const int e0 = b.nei_off[i], n = min(b.nei_off[i + 1] - e0, b.pad_cap);
+    const int2* row = b.pad + (size_t)i * b.pad_cap;
+    for (int q = lane; q < n; q += 32) {
+        const int2 v = row[q];
+        b.nei_j[e0 + q] = v.x;
+        b.nei_s[e0 + q] = v.y;
+    }
 }
 
 // Batches below this many atoms list neighbours with a warp per atom
@@ -452,10 +478,17 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, 
     ++L;
     k_sort_cells<<<(unsigned)((32LL * b.ncells + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     ++L;
-    if (warp_lists(b))
-        k_neighbours_warp<false><<<(unsigned)((32LL * b.natoms + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
-    else
-        k_neighbours<false><<<gA, kThreads, 0, s>>>(b, m);
+    const unsigned gW = (unsigned)((32LL * b.natoms + kThreads - 1) / kThreads);
+    if (b.pad_cap > 0) {  // plans: one search pass into padded rows
+        if (warp_lists(b))
+            k_neighbours_warp<2><<<gW, kThreads, 0, s>>>(b, m);
+        else
+            k_neighbours<2><<<gA, kThreads, 0, s>>>(b, m);
+    } else if (warp_lists(b)) {
+        k_neighbours_warp<0><<<gW, kThreads, 0, s>>>(b, m);
+    } else {
+        k_neighbours<0><<<gA, kThreads, 0, s>>>(b, m);
+    }
     ++L;
     L += launch_scan_from(b.nei_cnt, b.nei_off, b.natoms, b.scan_tmp, s);
     // status[1] = max count
@@ -468,10 +501,12 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, 
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) {
     const int gA = (b.natoms + kThreads - 1) / kThreads;
     const long long warps_threads = 32LL * b.natoms;
-    if (warp_lists(b))
-        k_neighbours_warp<true><<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
+    if (b.pad_cap > 0)
+        k_rows_to_lists<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
+    else if (warp_lists(b))
+        k_neighbours_warp<1><<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b, m);
     else
-        k_neighbours<true><<<gA, kThreads, 0, s>>>(b, m);
+        k_neighbours<1><<<gA, kThreads, 0, s>>>(b, m);
     // warps per atom: up to 8, until ~64 warps per SM of a B200 are in flight
     const int parts = (int)std::min<long long>(8, std::max<long long>(1, (148LL * 64 + b.natoms - 1) / std::max(b.natoms, 1)));
     const unsigned gR = (unsigned)((warps_threads * parts + kThreads - 1) / kThreads);

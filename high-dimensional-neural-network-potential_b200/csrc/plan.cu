@@ -319,6 +319,7 @@ int hdnnp_plan_create(hdnnp_model* m, const hdnnp_plan_opts* o, int nstruct, con
     if (!ok) return bail(HDNNP_E_CUDA, "plan buffers could not be allocated");
     if (p->pos_ref) k_fill<<<blocks((long long)n3), kThreads, 0, p->stream>>>(p->pos_ref, (long long)n3, INFINITY);
     p->pp.margin = o->margin;
+    p->pp.pad_lists = true;
     // molecules get their box on the device (periodic cells keep their set-up)
     p->pp.dev_boxes = false;
     for (int s = 0; s < nstruct; ++s) p->pp.dev_boxes = p->pp.dev_boxes || !periodic[s];
