@@ -127,6 +127,16 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // precision-dispatched math
 __device__ __forceinline__ double xsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
+// r and 1/r from r^2 > 0: FP64 by sqrt and division; FP32 by one reciprocal
+// square root (rsqrtf, 2 ulp) and a product
+__device__ __forceinline__ void dist_inv(double r2, double& r, double& ir) {
+    r = sqrt(r2);
+    ir = 1.0 / r;
+}
+__device__ __forceinline__ void dist_inv(float r2, float& r, float& ir) {
+    ir = rsqrtf(r2);
+    r = r2 * ir;
+}
 __device__ __forceinline__ double xexp(double x) { return exp(x); }
 // FP32 form: the exp2-based intrinsic (max error 2 + floor(1.173 |x|) ulp;
 // the angular arguments stay below ~5, where it is within 8 ulp)
@@ -585,8 +595,8 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
             const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;  // djk = r_j - r_k
             const T rjk2 = cx * cx + cy * cy + cz * cz;
-            const T rjk = xsqrt(rjk2);
-            const T irjk = (T)1 / rjk;
+            T rjk, irjk;
+            dist_inv(rjk2, rjk, irjk);
             const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk)), tt = tj * tj;
             const T fjk = tt * tj;
             const T dfjk = (T)(-3) * inv_rc * irjk * (tt - tt * tt);
