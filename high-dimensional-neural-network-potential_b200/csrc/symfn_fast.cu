@@ -137,6 +137,10 @@ __device__ __forceinline__ void dist_inv(float r2, float& r, float& ir) {
     ir = rsqrtf(r2);
     r = r2 * ir;
 }
+// a / b: FP64 by division; FP32 by the fast reciprocal-based form (2 ulp,
+// b between 2^-126 and 2^126)
+__device__ __forceinline__ double xdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double xexp(double x) { return exp(x); }
 // FP32 form: the exp2-based intrinsic (max error 2 + floor(1.173 |x|) ulp;
 // the angular arguments stay below ~5, where it is within 8 ulp)
@@ -324,7 +328,7 @@ __device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d
         cz = (double)b.z - (double)a.z;
     }
     const double D = rc2d - (cx * cx + cy * cy + cz * cz);
-    return D > 0.0 ? (T)D / (rc * (rc + rjk)) : (T)0;
+    return D > 0.0 ? xdiv((T)D, rc * (rc + rjk)) : (T)0;
 }
 
 // ---------------------------------------------------------------- grid specs
