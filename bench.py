@@ -258,7 +258,7 @@ def serve_leg(pkg, engine, pot, prec, seconds):
     """Served walkers: 256 ABX3 supercell walkers of 96-3072 atoms (seed 5),
     half velocity-Verlet MD (300 K, dt 20 a.u.), half Metropolis MC
     (N(0, 0.05 Bohr) trial moves), resident on the device in one server
-    (2 workers, 131,072-atom batches, 32 GB HBM budget).  A closed-loop
+    (3 workers, 131,072-atom batches, 32 GB HBM budget).  A closed-loop
     point (every idle walker steps at once) gives the saturated throughput;
     Poisson arrivals at 25/50/80 % of it give latency under load."""
     from hdnnp_b200 import server as S
@@ -266,7 +266,7 @@ def serve_leg(pkg, engine, pot, prec, seconds):
     W = pkg.workloads
     walkers = W.config_c5()
     budget = 32 << 30
-    srv = S.Server(pot, max_batch_atoms=131072, workers=2, precision=prec, hbm_budget=budget)
+    srv = S.Server(pot, max_batch_atoms=131072, workers=3, precision=prec, hbm_budget=budget)
     info = []
     for k, s in enumerate(walkers):
         md = k % 2 == 0
@@ -292,7 +292,7 @@ def serve_leg(pkg, engine, pot, prec, seconds):
     srv.close()
     nat = [w[1] for w in info]
     return {"workload": f"{len(info)} walkers, {min(nat)}-{max(nat)} atoms ({sum(nat)} total), half MD half MC",
-            "server": "2 workers, 131072-atom batches", "hbm_budget": budget, "hbm_charged": hbm,
+            "server": "3 workers, 131072-atom batches", "hbm_budget": budget, "hbm_charged": hbm,
             "saturation": sat, "poisson_sweep": sweep}
 
 
