@@ -768,6 +768,10 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if (c->profile && !pp) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // without the mid-pipeline host read, the structure a non-finite position
+    // blames comes back here (not inside a graph capture: plans read acc)
+    if (pp && pp->e_cap > 0 && capturing != cudaStreamCaptureStatusActive)
+        CUDA_TRY(cudaMemcpyAsync(c->h_status + 1, b.status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
     c->launches = L;
     c->last = b;
     c->have_last = true;
@@ -1370,6 +1374,12 @@ int ctx_profile_replay(hdnnp_ctx* c, long long evals, long long atoms) {
 
 // Device error flags of c's evaluations ([4] ints, flags in [0]).
 int* ctx_status_dev(hdnnp_ctx* c) { return c->status.p; }
+
+// Flags of the last evaluation on c as read back to the host (after its
+// stream was synchronised), and the largest neighbour count of the last
+// evaluation that read its counts on the host.
+int ctx_last_flags(hdnnp_ctx* c) { return c->h_status ? c->h_status[0] : 0; }
+int ctx_last_mmax(hdnnp_ctx* c) { return c->h_status ? c->h_status[3] : 0; }
 
 // Batch index of a structure with a non-finite position in the last
 // evaluation on c, or -1.

@@ -51,6 +51,8 @@ int eval_resident(hdnnp_ctx* c, int nstruct, const int64_t* off, const int32_t* 
 int ctx_list_arrays(hdnnp_ctx* c, size_t natoms, size_t nentries, CtxLists* out);
 int ctx_check_status(hdnnp_ctx* c);
 int ctx_bad_struct(hdnnp_ctx* c);
+int ctx_last_flags(hdnnp_ctx* c);
+int ctx_last_mmax(hdnnp_ctx* c);
 }  // namespace hdnnp
 
 using namespace hdnnp;
@@ -107,6 +109,10 @@ struct Request {
 struct Worker {
     hdnnp_ctx* ctx = nullptr;
     cudaStream_t stream = nullptr;
+    // largest per-atom neighbour count seen in a batch that counted its
+    // entries on the host (0: none yet); later batches that build their lists
+    // search once into padded rows of 1.25 x this + 8
+    int m_est = 0;
     std::thread th;
     double* pos = nullptr;  // batch arrays (device)
     int32_t* Z = nullptr;
@@ -156,16 +162,18 @@ struct hdnnp_server {
 namespace {
 
 // Worker workspace per batch atom: the context's FP64 and FP32 per-atom
-// arrays (G, dE/dG, positions, forces, virials ...), about 60 neighbour
-// entries of 12 B (index, shift, reverse) + 24 B (FP64 entry gradient) + 12 B
-// (FP32 copy), the batch arrays and pinned staging.
+// arrays (G, dE/dG, positions, forces, virials ...), about 100 neighbour
+// entries (batches that build their lists in one pass reserve 1.25 x the
+// densest atom + 8) of 12 B (index, shift, reverse) + 24 B (FP64 entry
+// gradient) + 12 B (FP32 copy) + 8 B (padded row), the batch arrays and
+// pinned staging.
 size_t workspace_bytes_per_atom(const hdnnp_model* m) {
     int nel = 0, zs[128], ns[128];
     double rc = 0;
     hdnnp_model_info(m, &nel, zs, ns, &rc);
     int nsf = 0;
     for (int e = 0; e < nel; ++e) nsf = std::max(nsf, ns[e]);
-    return (size_t)nsf * 24 + 60 * 48 + 400;
+    return (size_t)nsf * 24 + 100 * 56 + 400;
 }
 
 // Records a completion for hdnnp_server_next_done (server lock held).  Tickets
@@ -310,6 +318,16 @@ int evaluate_set(hdnnp_server* srv, Worker& w, const std::vector<std::pair<Reque
         pp.pos_ref = w.pos_ref;
         ppp = &pp;
     }
+    // lists built without a skin: one search pass into padded rows sized by
+    // the densest batch so far, no host read of the entry total
+    const int pad_cap = w.m_est > 0 ? ((int)std::ceil(1.25 * w.m_est) + 8 + 31) / 32 * 32 : 0;
+    const bool padded = mode == ListMode::Build && pad_cap > 0 && (double)off[n] * pad_cap < (double)INT32_MAX;
+    if (padded) {
+        pp.pad_lists = true;
+        pp.m_cap = pad_cap;
+        pp.e_cap = (long long)off[n] * pad_cap;
+        ppp = &pp;
+    }
     if (mode == ListMode::BuildKeep) {
         pp.rebuild = w.flag1;  // build, recording the wrap translations and reference positions
     } else if (mode == ListMode::Keep) {
@@ -352,6 +370,13 @@ int evaluate_set(hdnnp_server* srv, Worker& w, const std::vector<std::pair<Reque
         err = hdnnp_last_error();
         return status;
     }
+    if (padded && (ctx_last_flags(w.ctx) & 32)) {
+        // an atom with more neighbours than the padded rows hold: this batch
+        // again with its counts read on the host (results are not yet used)
+        w.m_est = 0;
+        return evaluate_set(srv, w, items, err, mode, ab, sb);
+    }
+    if (mode == ListMode::Build && !padded) w.m_est = std::max(w.m_est, ctx_last_mmax(w.ctx));
     if (mode == ListMode::BuildKeep) {
         // keep each walker's new list: offsets to the host, storage, copy-out
         CtxLists L{};

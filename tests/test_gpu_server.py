@@ -340,3 +340,30 @@ def test_skin_lists_match_rebuilt_lists(pot, S, W):
         assert st["built"] + st["kept"] == evals
         assert st["kept"] > 0 and len(walkers) < st["built"] < evals
         assert a.list_stats() == {"built": 0, "kept": 0}
+
+
+def test_denser_walker_than_the_padded_rows(pot, S, W, abx3_model):
+    """Batches that build their lists search once into padded rows sized by
+    the densest batch a worker has counted so far.  A walker denser than that
+    (the same cell compressed by 20 %: about twice the neighbours) overflows
+    the rows on the device; the batch is evaluated again with its counts read
+    on the host, and the result matches the oracle and a server that has seen
+    nothing sparser."""
+    rng = np.random.default_rng(61)
+    sparse = W.supercell(W.abx3_cell(), (2, 2, 2))
+    sparse["pos"] = sparse["pos"] + rng.normal(0.0, 0.1, sparse["pos"].shape)
+    dense = {"Z": sparse["Z"], "pos": sparse["pos"] * 0.8, "lat": sparse["lat"] * 0.8}
+    with S.Server(pot, max_batch_atoms=4096, workers=1) as srv:
+        a = srv.add_walker(sparse["Z"], sparse["pos"], sparse["lat"])
+        for _ in range(2):  # the first batch counts on the host, the second uses padded rows
+            srv.wait(srv.submit(a, S.REQ_EVAL))
+        b = srv.add_walker(dense["Z"], dense["pos"], dense["lat"])
+        E, F, dl, _ = srv.wait(srv.submit(b, S.REQ_EVAL))
+        E2, F2, dl2, _ = srv.wait(srv.submit(b, S.REQ_EVAL))  # padded rows now sized for it
+    with S.Server(pot, max_batch_atoms=4096, workers=1) as fresh:
+        c = fresh.add_walker(dense["Z"], dense["pos"], dense["lat"])
+        E0, F0, dl0, _ = fresh.wait(fresh.submit(c, S.REQ_EVAL))
+    assert E == E0 == E2 and np.array_equal(F, F0) and np.array_equal(F2, F0) and np.array_equal(dl, dl0)
+    ref = abx3_model.eval(dense["Z"], dense["pos"], dense["lat"])
+    assert abs(E - ref["energy"]) <= RTOL_E * abs(ref["energy"])
+    assert np.abs(F - ref["forces"]).max() <= ATOL_F
