@@ -196,7 +196,8 @@ struct hdnnp_ctx {
     DevBuf<unsigned> pairs;                               // contributing-pair lists (fast kernels)
     DevBuf<int> npairs;
     DevBuf<int> cnei_cnt, cnei_off, cnei_j, cnei_s, cnei_rev, cnei_map;  // compacted Verlet-skin lists
-    DevBuf<int> pad;                                      // padded neighbour rows of plans (int2 pairs)
+    DevBuf<int> pad;                                      // padded neighbour rows (int2 pairs)
+    int m_est = 0;  // largest neighbour count counted on the host by hdnnp_eval_batch (0: none yet)
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -621,7 +622,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     int L = 0;
     if (c->profile) {
         // a plan collects the stage times of its replays itself (ctx_profile_replay)
-        if (!pp && (r = collect_profile(c))) return r;
+        if ((!pp || pp->eager) && (r = collect_profile(c))) return r;
         for (auto& e : c->ev)
             if (!e) CUDA_TRY(cudaEventCreate(&e));
         if (!c->stats.p) {
@@ -629,7 +630,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             CUDA_TRY(cudaMemset(c->stats.p, 0, 8 * sizeof(unsigned long long)));
         }
         b.stats = c->stats.p;
-        if (!pp) {
+        if (!pp || pp->eager) {
             c->host_counts[0] += 1;
             c->host_counts[1] += natoms;
         }
@@ -765,7 +766,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
                : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
     if (cm) L += launch_committee_finish(b, *cm, c->cm_E.p, st);  // mean energies (and std)
     if ((r = mark(7))) return r;
-    if (c->profile && !pp) c->prof_pending = true;
+    if (c->profile && (!pp || pp->eager)) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     // without the mid-pipeline host read, the structure a non-finite position
@@ -925,12 +926,37 @@ int hdnnp_eval_batch(hdnnp_ctx* c, int nstruct, const int64_t* atom_off, const i
         return r;
     CUDA_TRY(cudaMemcpyAsync(c->Z.p, Z, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(c->pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    auto results = [&]() -> int {
+        CUDA_TRY(cudaMemcpyAsync(energy, c->energy.p, sizeof(double) * nstruct, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(force, c->force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
+        if (dEdLat)
+            CUDA_TRY(cudaMemcpyAsync(dEdLat, c->dEdLat.p, sizeof(double) * 9 * nstruct, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        return HDNNP_OK;
+    };
+    // After a call that counted its lists on the host, one search pass into
+    // padded rows of 1.25 x the densest atom seen + 8 (no host read inside
+    // the pipeline); an atom above that is flagged on the device, and the
+    // call runs again with counted lists before returning.
+    const int pad = c->m_est > 0 ? ((int)std::ceil(1.25 * c->m_est) + 8 + 31) / 32 * 32 : 0;
+    if (pad > 0 && (double)N * pad < (double)INT32_MAX) {
+        PipePlan lp{};
+        lp.eager = true;
+        lp.pad_lists = true;
+        lp.m_cap = pad;
+        lp.e_cap = (long long)N * pad;
+        if ((r = run_pipeline(c, nstruct, natoms, c->Z.p, c->pos.p, c->energy.p, c->force.p,
+                              dEdLat ? c->dEdLat.p : nullptr, st, &lp)) ||
+            (r = results()))
+            return r;
+        if (!(c->h_status[0] & 32)) return check_status(c);
+        if ((r = check_status(c))) return r;
+        c->m_est = 0;
+    }
     r = run_pipeline(c, nstruct, natoms, c->Z.p, c->pos.p, c->energy.p, c->force.p, dEdLat ? c->dEdLat.p : nullptr, st);
     if (r) return r;
-    CUDA_TRY(cudaMemcpyAsync(energy, c->energy.p, sizeof(double) * nstruct, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(force, c->force.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, st));
-    if (dEdLat) CUDA_TRY(cudaMemcpyAsync(dEdLat, c->dEdLat.p, sizeof(double) * 9 * nstruct, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    c->m_est = std::max(c->m_est, c->h_status[3]);  // the largest count, read by the pipeline
+    if ((r = results())) return r;
     return check_status(c);
 }
 
@@ -1054,6 +1080,9 @@ int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes) 
     else if (w == "nsf_max") { tmp = c->model->dev.nsf_max; n = sizeof(int); }
     else if (w == "nentries") { tmp = b.nentries; n = sizeof(int); }
     else return fail(HDNNP_E_INPUT, "unknown item " + w);
+    // list arrays: nentries is the reserved size (padded lists reserve more
+    // than they fill); the leading entries the caller sized for are copied
+    if (src && (src == b.nei_j || src == b.nei_s || src == b.nei_rev)) n = std::min(n, bytes);
     if (bytes < n) return fail(HDNNP_E_CAPACITY, "buffer too small");
     if (!src) {
         std::memcpy(host, &tmp, n);

@@ -206,6 +206,7 @@ struct PipePlan {
     double* wshift = nullptr;
     double* pos_ref = nullptr;
     bool pad_lists = false;  // one search pass into padded rows of m_cap (after the probe)
+    bool eager = false;      // an eager call (hdnnp_eval_batch): profiled like one
 };
 
 // Device neighbour-list arrays of a context (ctx_list_arrays in capi.cu).

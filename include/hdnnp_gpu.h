@@ -174,7 +174,10 @@ int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stre
  * row stride nsf_max), "dEdG" (same layout), "atom_energy" (nat),
  * "nei_count" (nat, excluding the atom itself), "nei_index" (entries),
  * "nei_shift" (entries, packed image shift), "nsf_max" (1 int).
- * `bytes` is the size of `host`; returns HDNNP_E_CAPACITY if too small.     */
+ * `bytes` is the size of `host`; returns HDNNP_E_CAPACITY if too small.  The
+ * list arrays ("nei_index", "nei_shift", "nei_rev") copy their first `bytes`
+ * (size the buffer from "nei_count"): their reserved size can exceed the
+ * entries filled.                                                             */
 int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes);
 
 /* Kernel launches issued by the last evaluation on `c`. */

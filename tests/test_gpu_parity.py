@@ -221,3 +221,32 @@ def test_compiled_and_runtime_zeta_kernels_agree(eng, gab, W):
     assert np.abs(fixed["energy"] - rt["energy"]).max() <= E_REL * np.abs(rt["energy"]).max()
     assert np.abs(fixed["forces"] - rt["forces"]).max() <= F_ABS
     assert np.abs(fixed["dEdLat"] - rt["dEdLat"]).max() <= L_ABS
+
+
+def test_denser_structure_after_a_sparse_one(eng, W, abx3_model):
+    """After a call that counted its lists on the host, hdnnp_eval_batch
+    searches once into padded rows sized by the densest atom seen so far.  A
+    denser structure (the same cell compressed by 20 %: about twice the
+    neighbours) overflows them on the device and the call runs again with
+    counted lists: the result equals a fresh context's bitwise and the
+    oracle's within the FP64 tolerances."""
+    rng = np.random.default_rng(62)
+    sparse = W.supercell(W.abx3_cell(), (2, 2, 2))
+    sparse["pos"] = sparse["pos"] + rng.normal(0.0, 0.1, sparse["pos"].shape)
+    dense = {"Z": sparse["Z"], "pos": sparse["pos"] * 0.8, "lat": sparse["lat"] * 0.8}
+    p = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        for _ in range(2):  # the first call counts on the host, the second uses padded rows
+            p.energy_and_forces(eng.AtStruct(sparse["Z"], sparse["pos"], sparse["lat"]), dEdLat=True)
+        E, F, dl = p.energy_and_forces(eng.AtStruct(dense["Z"], dense["pos"], dense["lat"]), dEdLat=True)
+        E2, F2, dl2 = p.energy_and_forces(eng.AtStruct(dense["Z"], dense["pos"], dense["lat"]), dEdLat=True)
+    finally:
+        p.close()
+    q = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        E0, F0, dl0 = q.energy_and_forces(eng.AtStruct(dense["Z"], dense["pos"], dense["lat"]), dEdLat=True)
+    finally:
+        q.close()
+    assert E == E0 == E2
+    assert np.array_equal(F, F0) and np.array_equal(F2, F0) and np.array_equal(dl, dl0) and np.array_equal(dl2, dl0)
+    check(E, F, dl, abx3_model.eval(dense["Z"], dense["pos"], dense["lat"]))
