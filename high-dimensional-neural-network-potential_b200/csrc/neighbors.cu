@@ -350,7 +350,10 @@ inline bool warp_lists(const Batch& b) {
 // of four entries; one search per group of 8 lanes, which scan j's list in
 // coalesced 8-entry chunks, the ballot picking the first match.  Small
 // batches use several warps per atom so that enough searches are in flight.
-template <bool kMulti>
+// kPad: the lists' padded rows are still in place (plans, eager calls after
+// the first): the search reads (j, shift) pairs as one 8-byte load from j's
+// row instead of two arrays; indices stay those of the CSR lists.
+template <bool kMulti, bool kPad>
 __global__ void k_reverse(Batch b, int parts) {
     const long long w = (long long)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     if (!kMulti) parts = 1;
@@ -360,18 +363,28 @@ __global__ void k_reverse(Batch b, int parts) {
     // four entries of atom a at a time, one per group of 8 lanes, so that the
     // dependent loads of four searches overlap
     const int grp = lane >> 3, gl = lane & 7;
-    const int e1 = b.nei_off[a + 1];
-    for (int e0 = b.nei_off[a] + 4 * part; e0 < e1; e0 += 4 * parts) {
+    const int ea = b.nei_off[a], e1 = b.nei_off[a + 1];
+    for (int e0 = ea + 4 * part; e0 < e1; e0 += 4 * parts) {
         const int e = e0 + grp;
         const bool live = e < e1;
         int want = 0, f0 = 0, f1 = 0;
+        const int2* row = nullptr;
         if (live) {
-            const int j = b.nei_j[e];
+            int j, sh;
+            if (kPad) {
+                const int2 v = b.pad[(size_t)a * b.pad_cap + (e - ea)];
+                j = v.x;
+                sh = v.y;
+            } else {
+                j = b.nei_j[e];
+                sh = b.nei_s[e];
+            }
             int sx, sy, sz;
-            unpack_shift(b.nei_s[e], sx, sy, sz);
+            unpack_shift(sh, sx, sy, sz);
             want = pack_shift(-sx, -sy, -sz);
             f0 = b.nei_off[j];
             f1 = b.nei_off[j + 1];
+            if (kPad) row = b.pad + (size_t)j * b.pad_cap;
         }
         int r = -1;
         // every iteration advances each open search by 8 entries of its list,
@@ -379,7 +392,15 @@ __global__ void k_reverse(Batch b, int parts) {
         for (int fb = 0;; fb += 8) {
             const int f = f0 + fb + gl;
             const bool open = live && r < 0 && f0 + fb < f1;
-            const bool hit = open && f < f1 && b.nei_j[f] == a && b.nei_s[f] == want;
+            bool hit = false;
+            if (open && f < f1) {
+                if (kPad) {
+                    const int2 v = row[fb + gl];
+                    hit = v.x == a && v.y == want;
+                } else {
+                    hit = b.nei_j[f] == a && b.nei_s[f] == want;
+                }
+            }
             const unsigned gm = (__ballot_sync(0xffffffffu, hit) >> (8 * grp)) & 0xffu;
             if (open && gm) r = f0 + fb + __ffs(gm) - 1;
             if (!__any_sync(0xffffffffu, live && r < 0 && f0 + fb + 8 < f1)) break;
@@ -510,10 +531,16 @@ int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) 
     // warps per atom: up to 8, until ~64 warps per SM of a B200 are in flight
     const int parts = (int)std::min<long long>(8, std::max<long long>(1, (148LL * 64 + b.natoms - 1) / std::max(b.natoms, 1)));
     const unsigned gR = (unsigned)((warps_threads * parts + kThreads - 1) / kThreads);
-    if (parts > 1)
-        k_reverse<true><<<gR, kThreads, 0, s>>>(b, parts);
-    else
-        k_reverse<false><<<gR, kThreads, 0, s>>>(b, 1);
+    if (b.pad_cap > 0) {
+        if (parts > 1)
+            k_reverse<true, true><<<gR, kThreads, 0, s>>>(b, parts);
+        else
+            k_reverse<false, true><<<gR, kThreads, 0, s>>>(b, 1);
+    } else if (parts > 1) {
+        k_reverse<true, false><<<gR, kThreads, 0, s>>>(b, parts);
+    } else {
+        k_reverse<false, false><<<gR, kThreads, 0, s>>>(b, 1);
+    }
     return 2;
 }
 
