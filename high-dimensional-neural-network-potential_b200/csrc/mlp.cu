@@ -16,12 +16,15 @@ namespace hdnnp {
 
 namespace {
 
+// Counts and slots per element with warp-aggregated atomics: the lanes of
+// one element in a warp add their number once (a handful of counters would
+// otherwise take one atomic per atom).  The order inside an element group is
+// that of the atomics; each atom's network output does not depend on it.
 __global__ void k_count_elements(Batch b, int nel) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < b.natoms) {
-        int e = b.elem[i];
-        if (e >= 0) atomicAdd(&b.el_count[e], 1);
-    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = i < b.natoms ? b.elem[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, e);
+    if (e >= 0 && (peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicAdd(&b.el_count[e], __popc(peers));
 }
 
 __global__ void k_element_starts(Batch b, int nel) {
@@ -37,14 +40,15 @@ __global__ void k_element_starts(Batch b, int nel) {
 }
 
 __global__ void k_fill_elements(Batch b) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < b.natoms) {
-        int e = b.elem[i];
-        if (e >= 0) {
-            int p = atomicAdd(&b.el_count[e], 1);
-            b.el_atoms[b.el_start[e] + p] = i;
-        }
-    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int e = i < b.natoms ? b.elem[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, e);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (e >= 0 && lane == leader) base = atomicAdd(&b.el_count[e], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (e >= 0) b.el_atoms[b.el_start[e] + base + __popc(peers & ((1u << lane) - 1u))] = i;
 }
 
 template <typename T>
