@@ -7,24 +7,33 @@ and N(0, 0.15 Bohr) jitter (seed 4 + rank), synthetic 5-element potential with
 280 symmetry functions per element and 280-25-25-1 networks
 (tests/golden/abx3).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
   python bench.py --impl reference ...   # the reference's algorithm on the host cores
 
 value  = atoms x steps / device time of the K steps (max over ranks), inputs
          resident in HBM, the batch as a resident plan (hdnnp_plan_*: one
          CUDA-graph launch per step, autotuned symmetry-function launches),
-         default precision "mixed" (FP32 symmetry functions, tensor-core
-         networks, FP64 wrap, energy and virial reductions).
+         default precision "fp64" (FP64 throughout, the arithmetic of the
+         reference), so that the ratio to the reference arm compares equal
+         arithmetic.
 e2e    = the same plan with pinned host buffers: H2D of Z/positions and D2H
          of energies/forces/dE/dh inside every step (wall clock, the stream
          synchronised each step); e2e.eager_one_call is the same through the
          one-call eager path (hdnnp_eval_batch, host set-up in every call).
-config.compare: the eager batched path (hdnnp_eval_batch_device), the
-         batched FP64 plan, the plain FP64 form (hdnnp_energy_and_forces, one
-         structure per call, the reference's API) on a sample of the
-         structures for the north-star ratio, the served walkers, and the
-         single-structure legs (methylammonium MD, 768-atom cell, 49,152-atom
-         MD) with the CPU stand-in beside each.
+error_vs_oracle: the largest errors of the timed plan's results against the
+         FP64 oracle on a seeded sample of 64 of its structures (and the same
+         for the mixed-precision plan in config.compare).
+config.compare: the mixed-precision form as a plan (FP32 symmetry
+         functions, tensor-core networks, FP64 wrap/energy/virial) with its
+         error against the oracle and its roofline, the eager batched path,
+         the plain FP64 form (hdnnp_energy_and_forces, one structure per call,
+         the reference's API) on a sample of the structures, both north-star
+         ratios, the served walkers (mixed), and the single-structure legs
+         (methylammonium MD, 768-atom cell, 49,152-atom MD) with the CPU
+         stand-in beside each.
+cpu_baseline / --impl reference: the oracle source (the reference's loops,
+         OpenMP over atoms) built g++ -O3 -march=native -fopenmp on the host
+         that runs the bench, on all its cores.
 """
 from __future__ import annotations
 
@@ -59,9 +68,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--structs", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=256, help="structures in the CPU baseline sample")
+    ap.add_argument("--error-sample", type=int, default=64, help="structures checked against the oracle")
     ap.add_argument("--plain-sample", type=int, default=512, help="structures timed through the plain per-structure API")
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="seconds per load point of the serving leg (0: skip)")
@@ -181,37 +191,134 @@ def measured_peaks(torch):
     return out
 
 
-# Floating-point operations per work unit of the lambda x zeta x eta
+# Floating-point operations per work unit EXECUTED by the lambda x zeta x eta
 # symmetry-function kernels for the (2 lambda, zeta {1,2,4,16}, 2 eta) grid of
 # this potential, counted from csrc/symfn_fast.cu (add/mul = 1, FMA = 2,
-# sqrt/exp/tanh/div = 1).  Units come from the engine's counters.
-FLOPS = {
+# sqrt/exp/tanh/div = 1).  Units come from the engine's counters.  The
+# product-space kernels execute about 9x fewer operations than the
+# reference's per-function loops; the roofline is therefore stated with the
+# algorithmic count below and the executed count beside it.
+FLOPS_EXECUTED = {
     "sf_values": {"entries": 30, "pairs": 88, "g2_terms": 6},
     "sf_gradients": {"entries": 57, "pairs": 263, "g2_terms": 13},
 }
 
+# Algorithmic operations per work unit of the reference's path (one value +
+# gradient evaluation), derived from the operation counts of
+# calcAllSymmetryFunctions (symmetryFunctions.f90:201-305) and the
+# contraction of hdnnpCalcNNs (hdnnps.f90:515-553): 30 per neighbour entry,
+# 20 per radial term, 90 per contributing angular pair (r_jk < rc), 100 per
+# angular term; the networks 4 x (multiply-adds of 280-25-25-1) = 30,600 per
+# atom.  Pairs with r_jk >= rc add exact zeros in the reference and are not
+# counted.
+FLOPS_ALGORITHMIC = {"entries": 30, "g2_terms": 20, "pairs": 90, "g4_terms": 100}
+MLP_FLOPS_PER_ATOM = 4 * (280 * 25 + 25 * 25 + 25)
 
-# DRAM bytes (read + write) per atom of each symmetry-function stage in the
-# mixed form, from one ncu capture of both launches of each kernel on the
-# first 1024 structures of this workload (191,160 atoms; values 706.5 MB,
-# gradients 842.5 MB), scaled by the atoms of a step: the traffic of these
-# kernels is per atom (positions, neighbour entries, G / dE/dG rows, pair
-# lists), so it grows in proportion.
-TRAFFIC_PER_ATOM = {"sf_values": 706.5e6 / 191160, "sf_gradients": 842.5e6 / 191160}
+# Algorithmic HBM bytes of the neighbour-list stages: positions and Z read
+# once (28 B per atom), each entry (4 B index + 4 B image code) written once
+# and read once (16 B per entry).
+LIST_BYTES = {"atoms": 28, "entries": 16}
+
+
+# DRAM bytes (read + write) per atom of each symmetry-function stage, from one
+# ncu capture of both launches of each kernel on the first 1024 structures of
+# this workload (191,160 atoms), scaled by the atoms of a step: the traffic of
+# these kernels is per atom (positions, neighbour entries, G / dE/dG rows,
+# pair lists), so it grows in proportion.
+TRAFFIC_PER_ATOM = {"mixed": {"sf_values": 706.5e6 / 191160, "sf_gradients": 842.5e6 / 191160}}
 
 
 def kernel_flops(stage, counters, evals):
-    per = FLOPS[stage]
+    per = FLOPS_EXECUTED[stage]
     return sum(per[k] * counters[k] for k in per) / max(evals, 1)
 
 
-def cpu_baseline(structs, sample, seed=0):
-    """The FP64 oracle (C++ restatement of the reference, OpenMP over atoms,
-    all host threads) on a seeded sample of the workload's structures."""
+def roofline(stage_ms, counters, peaks, precision, hbm_gbs):
+    """Roofline of the symmetry-function passes (the dominant pair of kernels,
+    k_sfv_fast + k_sfg_fast: ~80 % of a step), by the algorithmic count per
+    launch pair, with the executed count, the whole step and the list stages
+    beside it."""
+    evals = max(counters["evaluations"], 1)
+    per_step = {k: v / evals for k, v in counters.items() if k != "evaluations"}
+    ms = {k: v / evals for k, v in stage_ms.items()}
+    peak_key = "fp64" if precision == "fp64" else "fp32"
+    peak = peaks.get(peak_key)
+    sf_ms = ms["sf_values"] + ms["sf_gradients"]
+    alg = sum(FLOPS_ALGORITHMIC[k] * per_step[k] for k in FLOPS_ALGORITHMIC)
+    achieved = alg / (sf_ms / 1e3) / 1e12
+    step_ms = sum(ms.values())
+    step_alg = alg + MLP_FLOPS_PER_ATOM * per_step["atoms"]
+    list_ms = ms["neighbour_count"] + ms["neighbour_fill"]
+    list_bytes = sum(LIST_BYTES[k] * per_step[k] for k in LIST_BYTES)
+    executed = {}
+    for k in ("sf_values", "sf_gradients"):
+        f = kernel_flops(k, counters, evals)
+        a = f / (ms[k] / 1e3) / 1e12
+        executed[k] = {"flops_per_launch": f, "ms_per_launch": ms[k], "achieved_tflops": a,
+                       "frac": a / peak if peak else None}
+    tr = TRAFFIC_PER_ATOM.get(precision)
+    traffic = sum(tr[k] for k in tr) * per_step["atoms"] if tr else None
+    return {"bound": peak_key + "-alu", "kernel": "sf_values + sf_gradients (k_sfv_fast, k_sfg_fast)",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+            "flops_per_launch": alg, "ms_per_launch": sf_ms,
+            "flops_source": "algorithmic: 30 per entry + 20 per radial term + 90 per contributing angular pair + "
+                            "100 per angular term, times this step's unit counters",
+            "peak_source": f"measured in this run: cuBLAS {peak_key.upper()} GEMM (no TF32), best of 5 (of measured)",
+            "traffic": traffic, "traffic_unit": "bytes per step, DRAM read + write",
+            "traffic_source": "ncu capture of the same kernels on 1024 of the structures, scaled by atoms"
+            if traffic else "not captured for this precision",
+            "executed": executed,
+            "step": {"flops": step_alg, "ms": step_ms, "achieved_tflops": step_alg / (step_ms / 1e3) / 1e12,
+                     "frac": step_alg / (step_ms / 1e3) / 1e12 / peak if peak else None},
+            "lists": {"bytes": list_bytes, "ms": list_ms, "achieved_gbs": list_bytes / (list_ms / 1e3) / 1e9,
+                      "peak_gbs": hbm_gbs, "frac": list_bytes / (list_ms / 1e3) / 1e9 / hbm_gbs if hbm_gbs else None,
+                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_gbs else None},
+            "stage_ms_per_step": ms, "units_per_step": per_step}
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0  # fallback figure of this GPU pool
+
+
+def oracle_errors(plan, structs, n, seed=8):
+    """Largest errors of a plan's results against the FP64 oracle (checker
+    build) on a seeded sample of its structures."""
     from oracle import oracle as O
 
     O.set_threads(os.cpu_count() or 1)
-    m = O.Model(POT_DIR)
+    model = O.Model(POT_DIR)
+    E, F, D = plan.results()
+    idx = np.sort(np.random.default_rng(seed).choice(len(structs), min(n, len(structs)), replace=False))
+    out = {"dE_per_atom": 0.0, "dE_rel": 0.0, "dF_max": 0.0, "d_dEdLat_per_atom": 0.0, "d_dEdLat_max": 0.0}
+    for k in idx:
+        s = structs[int(k)]
+        ref = model.eval(s["Z"], s["pos"], s["lat"])
+        na = len(s["Z"])
+        a0, a1 = plan.off[k], plan.off[k + 1]
+        dE = abs(E[k] - ref["energy"])
+        out["dE_per_atom"] = max(out["dE_per_atom"], dE / na)
+        out["dE_rel"] = max(out["dE_rel"], dE / abs(ref["energy"]))
+        out["dF_max"] = max(out["dF_max"], float(np.abs(F[a0:a1] - ref["forces"]).max()))
+        dl = float(np.abs(D[k] - ref["dEdLat"]).max())
+        out["d_dEdLat_per_atom"] = max(out["d_dEdLat_per_atom"], dl / na)
+        out["d_dEdLat_max"] = max(out["d_dEdLat_max"], dl)
+    out["sample"] = f"{len(idx)} of the batch's structures (seed {seed}), FP64 oracle"
+    out["units"] = "Ha (energy), Ha/Bohr (forces), Ha (dE/dh)"
+    return out
+
+
+def cpu_baseline(structs, sample, seed=0):
+    """The oracle source (the C++ restatement of the reference, OpenMP over
+    atoms) built -O3 -march=native -fopenmp for this host, on all host
+    threads, on a seeded sample of the workload's structures."""
+    from oracle import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    m = O.Model(POT_DIR, native=True)
     rng = np.random.default_rng(seed)
     idx = rng.choice(len(structs), size=min(sample, len(structs)), replace=False)
     atoms = 0
@@ -222,6 +329,7 @@ def cpu_baseline(structs, sample, seed=0):
         atoms += len(s["Z"])
     dt = time.perf_counter() - t0
     return {"value": atoms / dt, "unit": "atom-steps/s", "cores": O.max_threads(), "kind": "port",
+            "build": O.NATIVE_FLAGS,
             "sample": f"{len(idx)} of the workload's structures ({atoms} atoms), one E+F+stress evaluation each, "
                       f"{dt:.1f} s"}
 
@@ -229,7 +337,8 @@ def cpu_baseline(structs, sample, seed=0):
 def run_reference(args, rank, world):
     """--impl reference: the reference's algorithm on the host cores.  The
     Fortran reference cannot be built in this image (no Fortran compiler), so
-    its C++ restatement (the oracle: same loops, OpenMP over atoms) runs it."""
+    its C++ restatement (the oracle: same loops, OpenMP over atoms), built
+    -O3 -march=native -fopenmp on this host, runs it."""
     if rank != 0:
         return
     W = __graft_entry__.load_package().workloads
@@ -249,14 +358,14 @@ def run_reference(args, rank, world):
             "config": {"workload": "batched mixed sizes: 4096 periodic ABX3 supercells (12-768 atoms), seed 4",
                        "step": "E+F+stress of a seeded sample of the structures (atom-steps/s is size-free)"},
             "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": base["cores"], "kind": "port",
-                             "sample": base["sample"]},
+                             "build": base["build"], "sample": base["sample"]},
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def serve_leg(pkg, engine, pot, prec, seconds):
     """Served walkers: 256 ABX3 supercell walkers of 96-3072 atoms (seed 5),
-    half velocity-Verlet MD (300 K, dt 20 a.u.), half Metropolis MC
+    half velocity-Verlet MD (300 K, dt DT_SYNTH = 0.5 a.u.), half Metropolis MC
     (N(0, 0.05 Bohr) trial moves), resident on the device in one server
     (3 workers, 131,072-atom batches, 32 GB HBM budget).  A closed-loop
     point (every idle walker steps at once) gives the saturated throughput;
@@ -620,7 +729,11 @@ def main():
 
     # ---------------- comparisons on the same workload (rank 0)
     compare = {}
+    errors = {}
+    peaks = measured_peaks(torch) if rank == 0 else {}
+    hbm = hbm_peak()
     if rank == 0:
+        errors[args.precision] = oracle_errors(bplan, structs, args.error_sample)
         nk = max(2, args.steps // 3)
         # the same precision without the graph (host set-up + one host read per step)
         step_eager()
@@ -628,13 +741,23 @@ def main():
         et = timed_device_steps(nk, fn=step_eager)
         torch.cuda.synchronize()
         compare["batched_eager_" + args.precision] = natoms * len(et) / (sum(a.elapsed_time(b) for a, b in et) / 1e3)
-        # the other precision, as a plan
+        # the other precision, as an autotuned plan, with its own roofline and error
         other = engine.HDNNP_PREC_FP64 if prec == engine.HDNNP_PREC_MIXED else engine.HDNNP_PREC_MIXED
-        oplan = PLm.Plan(pot, structs, precision=other, margin=0.02)
-        ot = timed_device_steps(nk, fn=lambda: oplan.launch(stream.cuda_stream))
+        oname = "fp64" if other == engine.HDNNP_PREC_FP64 else "mixed"
+        oplan = PLm.Plan(pot, structs, precision=other, margin=0.02, profile=True, autotune=True)
+        for _ in range(args.warmup):
+            oplan.launch(stream.cuda_stream)
+        oplan.sync(stream.cuda_stream)
+        oplan.profile(reset=True)
+        ot = timed_device_steps(max(nk, args.steps // 2), plan=oplan)
         oplan.sync(stream.cuda_stream)
         osec = sum(a.elapsed_time(b) for a, b in ot) / 1e3
-        compare["batched_" + ("fp64" if other == engine.HDNNP_PREC_FP64 else "mixed")] = natoms * len(ot) / osec
+        ost, ocnt = oplan.profile(reset=True)
+        compare["batched_" + oname] = natoms * len(ot) / osec
+        compare["batched_" + oname + "_ms_per_step"] = osec / len(ot) * 1e3
+        compare["batched_" + oname + "_roofline"] = roofline(ost, ocnt, peaks, oname, hbm)
+        compare["batched_" + oname + "_autotuned"] = oplan.tuning()
+        errors[oname] = oracle_errors(oplan, structs, args.error_sample)
         oplan.close()
         pot.set_precision(engine.HDNNP_PREC_FP64)
         rng = np.random.default_rng(7)
@@ -648,34 +771,26 @@ def main():
         psec = time.perf_counter() - t0
         compare["plain_fp64_per_structure"] = atoms / psec
         compare["plain_sample"] = f"{len(sample)} structures ({atoms} atoms), hdnnp_energy_and_forces with host arrays"
-        compare["value_over_plain_fp64"] = value / compare["plain_fp64_per_structure"]
+        mixed_v = value if args.precision == "mixed" else compare["batched_mixed"]
+        fp64_v = value if args.precision == "fp64" else compare["batched_fp64"]
+        compare["north_star"] = {
+            "target": "batched/served mixed >= 5x the plain FP64 GPU path on the same mixed-size workload",
+            "mixed_over_plain_fp64_per_structure": mixed_v / compare["plain_fp64_per_structure"],
+            "mixed_over_batched_fp64": mixed_v / fp64_v,
+            "batched_fp64_over_plain_fp64_per_structure": fp64_v / compare["plain_fp64_per_structure"]}
         pot.set_precision(prec)
         if world == 1 and args.serve_seconds > 0:
-            compare["served"] = serve_leg(pkg, engine, pot, prec, args.serve_seconds)
-            compare["served_over_plain_fp64"] = (compare["served"]["saturation"]["atom_steps_per_s"]
-                                                 / compare["plain_fp64_per_structure"])
+            pot.set_precision(engine.HDNNP_PREC_MIXED)
+            compare["served"] = serve_leg(pkg, engine, pot, engine.HDNNP_PREC_MIXED, args.serve_seconds)
+            compare["served"]["precision"] = "mixed"
+            compare["north_star"]["served_mixed_over_plain_fp64_per_structure"] = (
+                compare["served"]["saturation"]["atom_steps_per_s"] / compare["plain_fp64_per_structure"])
+            pot.set_precision(prec)
         if world == 1 and args.md:
             compare.update(md_legs(pkg, engine, PLm, pot, torch))
 
-    # ---------------- roofline of the dominant kernel
-    evals = max(counters["evaluations"], 1)
-    dom = max(("sf_values", "sf_gradients"), key=lambda k: stage_ms[k])
-    dom_ms = stage_ms[dom] / evals
-    flops = kernel_flops(dom, counters, evals)
-    peaks = measured_peaks(torch) if rank == 0 else {}
-    peak_key = "fp64" if args.precision == "fp64" else "fp32"
-    achieved = flops / (dom_ms / 1e3) / 1e12
-    traffic = TRAFFIC_PER_ATOM[dom] * counters["atoms"] / evals if args.precision == "mixed" else None
-    roof = {"bound": peak_key + "-alu", "kernel": dom, "achieved": achieved, "peak": peaks.get(peak_key),
-            "unit": "TFLOP/s", "frac": achieved / peaks[peak_key] if peaks.get(peak_key) else None,
-            "peak_source": f"measured in this run: cuBLAS {peak_key.upper()} GEMM (no TF32), best of 5",
-            "traffic": traffic, "traffic_unit": "bytes per step, DRAM read + write",
-            "traffic_source": "ncu capture of the same kernel on 1024 of the structures, scaled by atoms"
-            if traffic else "not captured for this precision",
-            "dram_GBs": traffic / (dom_ms / 1e3) / 1e9 if traffic else None,
-            "flops_per_launch": flops, "ms_per_launch": dom_ms,
-            "stage_ms_per_step": {k: v / evals for k, v in stage_ms.items()},
-            "units_per_step": {k: v / evals for k, v in counters.items() if k != "evaluations"}}
+    # ---------------- roofline of the dominant kernels (the two SF passes)
+    roof = roofline(stage_ms, counters, peaks, args.precision, hbm)
 
     if world > 1:
         dist.barrier()
@@ -692,8 +807,10 @@ def main():
                            "parallelism": f"replicas x{world} (independent structures per GPU)",
                            "autotuned": bplan.tuning(),
                            "l2": "256 MB buffer written between timed steps; working set (G alone "
-                                 f"{natoms * 280 * 4 / 1e9:.1f}+ GB) is larger than L2",
+                                 f"{natoms * 280 * (8 if args.precision == 'fp64' else 4) / 1e9:.1f}+ GB) "
+                                 "is larger than L2",
                            "compare": compare},
+                "error_vs_oracle": errors,
                 "e2e": {"value": e2e, "unit": "atom-steps/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h),
                         "path": "resident plan: H2D of Z and positions, graph launch, D2H of E, F, dE/dh",

@@ -1134,18 +1134,23 @@ int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches) {
 
 // ====================================================================== no-allocation entry point
 // hdnnp_energy_and_forces_noalloc: the evaluation of hdnnp_energy_and_forces
-// for callers that cannot allocate GPU memory at evaluation time, such as a
-// host code that runs under a fixed memory budget handed out at start-up,
-// code running inside someone else's stream capture, or a language binding
-// without access to the CUDA allocator.  All intermediates live in one
-// static device array instead of a context workspace; inputs and outputs are
-// the caller's host arrays, as for hdnnp_energy_and_forces.
+// for callers that cannot allocate GPU memory at evaluation time, such as an
+// MD or Monte Carlo host code that runs under a fixed device-memory budget
+// handed out at start-up, or a language binding without access to the CUDA
+// allocator.  All intermediates live in one static device array instead of a
+// context workspace; inputs and outputs are the caller's host arrays, as for
+// hdnnp_energy_and_forces.  It copies synchronously on the legacy default
+// stream, so it must not run while any stream of the device is being captured
+// in the global capture mode (those copies would end that capture).
 #include <mutex>
 
 namespace {
 
-// Size of the static scratch.  Every GPU that loads the library's code for
-// this entry point keeps these bytes reserved until the process exits.
+// Size of the static scratch.  The array is part of the library's device
+// code: under lazy module loading (CUDA's default) a device reserves it when
+// this entry point first runs there; with CUDA_MODULE_LOADING=EAGER every
+// device the process initialises reserves it when the library is loaded.
+// Either way it stays reserved until the process exits.
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 constexpr int kNoAllocMaxDevices = 64;
 
@@ -1164,6 +1169,17 @@ int noalloc_setup(int dev) {
     if (e != cudaSuccess)
         return fail(HDNNP_E_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
     g_noalloc_ptr[dev] = (unsigned char*)p;
+    return HDNNP_OK;
+}
+
+// Device error flags of a no-allocation call, mapped as for a context
+// (check_status); the structure index of flag 8 is always 0 here.
+int noalloc_flags(int f) {
+    if (f & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
+    if (f & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
+    if (f & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
+    if (f & 8) return fail(HDNNP_E_INPUT, "non-finite position");
+    if (f & 16) return fail(HDNNP_E_TIMEOUT, "bounded wait expired");
     return HDNNP_OK;
 }
 
@@ -1196,6 +1212,15 @@ extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, co
     const int dev = m->device;
     if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HDNNP_E_INPUT, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mu[dev]);
+    // the caller's current device is restored on every return
+    int caller_dev = -1;
+    CUDA_TRY(cudaGetDevice(&caller_dev));
+    struct RestoreDevice {
+        int d;
+        ~RestoreDevice() {
+            if (d >= 0) cudaSetDevice(d);
+        }
+    } restore{caller_dev};
     CUDA_TRY(cudaSetDevice(dev));
     int r = noalloc_setup(dev);
     if (r) return r;
@@ -1267,9 +1292,9 @@ extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, co
     CUDA_TRY(cudaMemcpy(&h[0], b.status, sizeof(int), cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(&h[1], b.nei_off + nat, sizeof(int), cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(&h[2], b.status + 1, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h[0] & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
-    if (h[0] & 8) return fail(HDNNP_E_INPUT, "non-finite position");
-    const size_t E = (size_t)std::max(h[1], 0);
+    if ((r = noalloc_flags(h[0]))) return r;
+    if (h[1] < 0) return fail(HDNNP_E_CAPACITY, "more than 2^31 neighbour entries");
+    const size_t E = (size_t)h[1];
     b.nentries = (int)E;
     b.mmax = h[2];
     b.nei_j = cv.take<int>(E + 1);
@@ -1297,9 +1322,7 @@ extern "C" int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, co
     CUDA_TRY(cudaMemcpy(force, Fd, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost));
     if (dEdLat) CUDA_TRY(cudaMemcpy(dEdLat, Ld, sizeof(double) * 9, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(&h[0], b.status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h[0] & 2) return fail(HDNNP_E_STATE, "internal error: neighbour list is not symmetric");
-    if (h[0] & 4) return fail(HDNNP_E_CAPACITY, "neighbour count above the kernel capacity");
-    return HDNNP_OK;
+    return noalloc_flags(h[0]);
 }
 
 // ====================================================================== internal (C++) entry points of the server

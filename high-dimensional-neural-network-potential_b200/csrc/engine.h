@@ -291,6 +291,7 @@ int launch_committee_finish(const Batch& b, const Committee& cm, const double* E
 size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
+int device_sm_count();  // multiprocessors of the current device (cached per device)
 size_t small_md_smem_bytes(const DevModel& m, int natoms);  // dynamic shared memory of the kernel
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& a, cudaStream_t s);
 

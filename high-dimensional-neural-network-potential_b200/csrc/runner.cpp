@@ -13,8 +13,13 @@
 // Hardening over the reference (which prints and stops): errors are
 // returned; no cap of 200 symmetry functions per element; symmetry-function
 // types other than 2 and 3 and inconsistent network sizes are rejected;
-// 'cutoff_type' is read but, as in the reference, the tanh^3 cutoff of
-// symmetryFunctions.f90:310-327 is always used.
+// 'cutoff_type' must be 2 when it is given.  The reference ignores the
+// keyword and always evaluates the tanh^3 cutoff of
+// symmetryFunctions.f90:310-327, which is RuNNer's cutoff_type 2 (the
+// reference's own example, example/hdnnp-params/input.nn:70); a potential
+// trained with another cutoff would load there without complaint and give
+// wrong energies and forces, so it is refused here.  A file without the
+// keyword loads, as in the reference.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -126,6 +131,12 @@ bool load_runner(const std::string& dir_in, HostModel& m, std::string& err) {
             int z = w.size() >= 3 ? symbol_to_z(w[1]) : -1;
             if (z < 1 || !to_real(w[2], e)) return bad("bad atom_energy");
             atom_e[z] = e;
+        } else if (key == "cutoff_type") {
+            int ct = -1;
+            if (w.size() < 2 || !to_int(w[1], ct)) return bad("bad cutoff_type");
+            if (ct != 2)
+                return bad("cutoff_type " + w[1] +
+                           " is not supported: the symmetry functions use the tanh^3 cutoff (cutoff_type 2)");
         } else if (key == "scale_symmetry_functions") {
             m.scalesf = true;
         } else if (key == "center_symmetry_functions") {

@@ -30,6 +30,7 @@
 //    (3 doubles), the centre term g_self = -sum_e g_e and the atom virial
 //    W_i = -sum_e g_e (x) d_e, which the force gather and the structure
 //    reduction consume.
+#include <atomic>
 #include <cstdio>
 
 #include "engine.h"
@@ -58,25 +59,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_sf_gradients(Batch b, D
     }
 }
 
-int num_sms() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+int num_sms() { return device_sm_count(); }
 
 template <int GM>
 void launch_values_gm(const Batch& b, const DevModel& m, int mm, cudaStream_t st) {
     size_t smem = warp_bytes<double>(mm, m.nsf_max, false) * kWarpsPerBlock;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_sf_values<GM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
+    // set on every launch: the attribute is per device, and calls come from several threads
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_sf_values<GM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = (b.natoms + kWarpsPerBlock - 1) / kWarpsPerBlock;
     int cap = num_sms() * 16;
     if (blocks > cap) blocks = cap;
@@ -104,17 +93,30 @@ int launch_sf_values(const Batch& b, const DevModel& m, cudaStream_t st) {
 int launch_sf_gradients(const Batch& b, const DevModel& m, cudaStream_t st) {
     const int mm = ((b.mmax + 31) / 32) * 32 > 0 ? ((b.mmax + 31) / 32) * 32 : 32;
     size_t smem = warp_bytes<double>(mm, m.nsf_max, true) * kWarpsPerBlock;
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-        cudaFuncSetAttribute(k_sf_gradients, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = smem;
-    }
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_sf_gradients, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = (b.natoms + kWarpsPerBlock - 1) / kWarpsPerBlock;
     int cap = num_sms() * 16;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     k_sf_gradients<<<blocks, 32 * kWarpsPerBlock, smem, st>>>(b, m, mm);
     return 1;
+}
+
+// Multiprocessor count of the current device, cached per device ordinal
+// (contexts on several devices and several host threads call this).
+int device_sm_count() {
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> cache[kMaxDev];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    if (dev >= 0 && dev < kMaxDev) {
+        const int c = cache[dev].load(std::memory_order_relaxed);
+        if (c > 0) return c;
+    }
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    if (dev >= 0 && dev < kMaxDev) cache[dev].store(n, std::memory_order_relaxed);
+    return n;
 }
 
 }  // namespace hdnnp

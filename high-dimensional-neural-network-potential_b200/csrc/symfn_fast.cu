@@ -840,16 +840,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
     }
 }
 
-int nsm() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+int nsm() { return device_sm_count(); }
 
 template <typename K>
 void set_smem(K kernel, size_t smem) {

@@ -142,24 +142,30 @@ int hdnnp_committee_eval_batch(hdnnp_ctx* c, hdnnp_model* const* members, int nm
  * hdnnp_energy_and_forces (host arrays in and out, same arguments and
  * results), for callers that cannot allocate GPU memory when they evaluate:
  * an MD or Monte Carlo host code that runs under a fixed device-memory budget
- * handed out at start-up, code that runs inside another library's stream
- * capture (where cudaMalloc is not allowed), or a language binding without
- * access to the CUDA allocator.  It needs no context and calls no cudaMalloc,
- * cudaFree or allocating library routine: all intermediates live in one
- * static 32 MiB device array compiled into the library, which every GPU that
- * runs this entry point keeps reserved until the process exits.
+ * handed out at start-up, or a language binding without access to the CUDA
+ * allocator.  It needs no context and calls no cudaMalloc, cudaFree or
+ * allocating library routine: all intermediates live in one static 32 MiB
+ * device array compiled into the library.
+ * Memory: under lazy module loading (CUDA's default) a device reserves the
+ * 32 MiB when this entry point first runs on it, so make that first call at
+ * start-up, before a memory budget is handed out; with
+ * CUDA_MODULE_LOADING=EAGER every process that loads the library reserves
+ * them on every device it initialises.  The array stays reserved until the
+ * process exits.
  * Limit: the structure must fit that array (for a 280-SF potential about
  * 5,000 atoms with ~52 neighbours each; in general about
  * nat * (16 * nsf_max + 210) + neighbour_entries * 36 bytes); larger inputs
  * return HDNNP_E_CAPACITY with the size that did not fit.
  * Set-up: the first call on a device looks up the device address of the
- * static array (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.
+ * static array (cudaGetSymbolAddress) with that device current.
+ * Streams: the call copies synchronously and runs its kernels on the legacy
+ * default stream, and returns when they are done.  It must not run while any
+ * stream of the device is being captured in the global capture mode.  The
+ * caller's current device is restored before it returns.
  * Sharing: every call uses the same array and it keeps the last call's
  * contents (the call clears what must start at zero).  Calls are serialised
  * per device inside one process; calls that overlap on the GPU from other
- * processes or other copies of the library race on the array.  The work runs
- * on the legacy default stream and the call returns when it is done.        */
+ * processes or other copies of the library race on the array.               */
 int hdnnp_energy_and_forces_noalloc(const hdnnp_model* m, int nat, const int32_t* Z, const double* pos,
                                     int periodic, const double* lat, double* energy, double* force,
                                     double* dEdLat);

@@ -12,6 +12,8 @@ import __graft_entry__  # noqa: E402
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 EXAMPLE_DIR = os.path.join(GOLDEN, "example")
 ABX3_DIR = os.path.join(GOLDEN, "abx3")
+# softplus/ReLU layers and non-integer zeta (tests/golden/make_prz_potential.py)
+PRZ_DIR = os.path.join(GOLDEN, "prz")
 
 
 def pytest_configure(config):
@@ -43,6 +45,11 @@ def ex_model(orc):
 @pytest.fixture(scope="session")
 def abx3_model(orc):
     return orc.Model(ABX3_DIR)
+
+
+@pytest.fixture(scope="session")
+def prz_model(orc):
+    return orc.Model(PRZ_DIR)
 
 
 @pytest.fixture(scope="session")

@@ -61,6 +61,38 @@ def test_parser_errors_are_status_codes(eng, tmp_path):
     assert code == 2 and "scaling.data" in msg
 
 
+def _copy_example(tmp_path, name, edit):
+    d = tmp_path / name
+    d.mkdir()
+    for f in os.listdir(EXAMPLE_DIR):
+        (d / f).write_bytes(open(os.path.join(EXAMPLE_DIR, f), "rb").read())
+    (d / "input.nn").write_text(edit((d / "input.nn").read_text()))
+    return str(d)
+
+
+def test_cutoff_type_other_than_tanh3_is_refused(eng, tmp_path):
+    """The reference always evaluates tanh^3 (symmetryFunctions.f90:310-327),
+    RuNNer's cutoff_type 2, whatever input.nn says; another value is refused
+    with an I/O status instead of loading a potential that would give wrong
+    forces.  Type 2 and a file without the keyword get past the parser (on a
+    machine without a GPU they then fail at the device upload, status 5)."""
+    import torch
+
+    for bad in ("1", "0", "3"):
+        d = _copy_example(tmp_path, "ct" + bad, lambda s, b=bad: s.replace("cutoff_type 2", "cutoff_type " + b))
+        code, msg, _ = _load(eng, d)
+        assert code == 2 and "cutoff_type " + bad in msg and "tanh^3" in msg, (code, msg)
+    d = _copy_example(tmp_path, "ctjunk", lambda s: s.replace("cutoff_type 2", "cutoff_type x"))
+    code, msg, _ = _load(eng, d)
+    assert code == 2 and "cutoff_type" in msg
+    ok_codes = (0,) if torch.cuda.is_available() else (5,)
+    for name, edit in (("ct2", lambda s: s), ("ctnone", lambda s: s.replace("cutoff_type 2", ""))):
+        code, msg, h = _load(eng, _copy_example(tmp_path, name, edit))
+        assert code in ok_codes, (name, code, msg)
+        if code == 0:
+            eng.lib().hdnnp_model_free(h)
+
+
 def test_no_cpu_fallback_without_gpu(eng):
     import torch
 

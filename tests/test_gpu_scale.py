@@ -1,0 +1,134 @@
+"""Parity at the sizes the benchmark times, against the FP64 oracle.
+
+* The strained 49,152-atom cell (16x16x16 ABX3, 3 % triclinic strain, seed 2):
+  one eager FP64 evaluation (|dE| <= 1e-10 |E|, max |dF| and max |d dE/dh|
+  <= 1e-9) and one eager mixed one; then the benchmark's own form of it: a
+  mixed-precision MD plan with a 1 Bohr Verlet skin (300 K, seed 3, dt 0.5
+  a.u., 20 steps per launch), whose forces and dE/dh after 40 steps are
+  compared with the oracle at the plan's own positions.
+* The 4096-structure batch of the benchmark (nx, ny, nz in 1..4, seed 4;
+  758,676 atoms) as an autotuned resident plan in both precisions: a seeded
+  sample of 64 of its structures against the oracle.
+
+Mixed-precision budget (north star): |dE| per atom <= 1e-6 Ha, max |dF| <=
+1e-5 Ha/Bohr, |d dE/dh| per atom <= 1e-5.  Measured errors are printed.
+"""
+import numpy as np
+import pytest
+
+from conftest import ABX3_DIR
+
+pytestmark = pytest.mark.gpu
+
+E_REL, F_ABS, L_ABS = 1e-10, 1e-9, 1e-9
+E_ATOM, F_MIX, L_ATOM = 1e-6, 1e-5, 1e-5
+
+
+@pytest.fixture(scope="module")
+def eng(pkg):
+    from hdnnp_b200 import engine
+
+    return engine
+
+
+@pytest.fixture(scope="module")
+def c3(W):
+    return W.config_c3()
+
+
+@pytest.fixture(scope="module")
+def c3_ref(c3, abx3_model, orc):
+    import os
+
+    orc.set_threads(os.cpu_count() or 1)
+    return abx3_model.eval(c3["Z"], c3["pos"], c3["lat"])
+
+
+def test_strained_49152_fp64_and_mixed(eng, c3, c3_ref):
+    pot = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        ats = eng.AtStruct(c3["Z"], c3["pos"], c3["lat"])
+        E, F, dl = pot.energy_and_forces(ats, dEdLat=True)
+        n = len(c3["Z"])
+        print(f"C3 FP64: |dE|/|E| {abs(E - c3_ref['energy']) / abs(c3_ref['energy']):.2e}  "
+              f"max|dF| {np.abs(F - c3_ref['forces']).max():.2e}  max|d dEdLat| {np.abs(dl - c3_ref['dEdLat']).max():.2e}")
+        assert abs(E - c3_ref["energy"]) <= E_REL * abs(c3_ref["energy"])
+        assert np.abs(F - c3_ref["forces"]).max() <= F_ABS
+        assert np.abs(dl - c3_ref["dEdLat"]).max() <= L_ABS
+        pot.set_precision(eng.HDNNP_PREC_MIXED)
+        E, F, dl = pot.energy_and_forces(ats, dEdLat=True)
+        eE, eF, eL = abs(E - c3_ref["energy"]) / n, np.abs(F - c3_ref["forces"]).max(), \
+            np.abs(dl - c3_ref["dEdLat"]).max() / n
+        print(f"C3 mixed: |dE|/atom {eE:.2e}  max|dF| {eF:.2e}  |d dEdLat|/atom {eL:.2e}")
+        assert eE <= E_ATOM and eF <= F_MIX and eL <= L_ATOM
+    finally:
+        pot.close()
+
+
+def test_strained_49152_md_with_skin_matches_oracle(pkg, W, eng, c3, abx3_model):
+    from hdnnp_b200 import plan as PL
+
+    m3, p3 = W.maxwell_boltzmann(c3["Z"], 300.0, 3)
+    pot = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        with PL.Plan(pot, [c3], precision=eng.HDNNP_PREC_MIXED, skin=1.0, masses=m3, momenta=p3, dt=0.5,
+                     steps_per_launch=20, want_dEdLat=True) as pl:
+            builds = 0
+            for _ in range(2):
+                pl.launch()
+                builds += pl.sync()
+            E, F, D = pl.results()
+            pos = pl.pos.cpu().numpy()
+    finally:
+        pot.close()
+    ref = abx3_model.eval(c3["Z"], pos, c3["lat"])
+    n = len(c3["Z"])
+    eE, eF, eL = abs(E[0] - ref["energy"]) / n, np.abs(F - ref["forces"]).max(), np.abs(D[0] - ref["dEdLat"]).max() / n
+    moved = np.abs(pos - c3["pos"]).max()
+    print(f"C3 MD (mixed, 1 Bohr skin, 40 steps, {builds} list builds, max displacement {moved:.3f} Bohr): "
+          f"|dE|/atom {eE:.2e}  max|dF| {eF:.2e}  |d dEdLat|/atom {eL:.2e}")
+    assert moved > 0.0
+    assert eE <= E_ATOM and eF <= F_MIX and eL <= L_ATOM
+
+
+def _sample_errors(plan, structs, idx, model):
+    E, F, D = plan.results()
+    eE = eF = eL = 0.0
+    rE = rF = rL = 0.0
+    for k in idx:
+        s = structs[k]
+        ref = model.eval(s["Z"], s["pos"], s["lat"])
+        n = len(s["Z"])
+        a0, a1 = plan.off[k], plan.off[k + 1]
+        eE = max(eE, abs(E[k] - ref["energy"]) / n)
+        rE = max(rE, abs(E[k] - ref["energy"]) / abs(ref["energy"]))
+        eF = max(eF, np.abs(F[a0:a1] - ref["forces"]).max())
+        eL = max(eL, np.abs(D[k] - ref["dEdLat"]).max() / n)
+        rL = max(rL, np.abs(D[k] - ref["dEdLat"]).max())
+    return {"dE_atom": eE, "dE_rel": rE, "dF": eF, "dL_atom": eL, "dL": rL}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bench_batch_4096_sample(pkg, W, eng, abx3_model, orc, precision):
+    import os
+
+    from hdnnp_b200 import plan as PL
+
+    orc.set_threads(os.cpu_count() or 1)
+    structs = W.config_c4(n_struct=4096, seed=4)
+    prec = eng.HDNNP_PREC_FP64 if precision == "fp64" else eng.HDNNP_PREC_MIXED
+    idx = np.sort(np.random.default_rng(8).choice(len(structs), 64, replace=False))
+    pot = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        with PL.Plan(pot, structs, precision=prec, margin=0.02, autotune=True) as pl:
+            pl.launch()
+            pl.sync()
+            err = _sample_errors(pl, structs, idx, abx3_model)
+    finally:
+        pot.close()
+    print(f"4096-structure batch ({precision}, 64-structure sample): " +
+          "  ".join(f"{k} {v:.2e}" for k, v in err.items()))
+    if precision == "fp64":
+        assert err["dE_rel"] <= E_REL and err["dF"] <= F_ABS and err["dL"] <= L_ABS
+    else:
+        assert err["dE_atom"] <= E_ATOM and err["dF"] <= F_MIX and err["dL_atom"] <= L_ATOM

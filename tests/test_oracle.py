@@ -105,14 +105,19 @@ def test_fd_forces_and_dEdLat_small_cell(abx3_model, W):
     assert np.abs(fdl - r["dEdLat"]).max() < 1e-8 * max(1.0, np.abs(r["dEdLat"]).max())
 
 
-@pytest.mark.parametrize("case", ["example", "small_cell"])
-def test_independent_autograd(case, ex_model, abx3_model, c1, W):
+@pytest.mark.parametrize("case", ["example", "small_cell", "prz_cell"])
+def test_independent_autograd(case, ex_model, abx3_model, prz_model, c1, W):
+    """prz_cell: softplus/ReLU layers and non-integer zeta (the real-power
+    branch, symmetryFunctions.f90:266-273; activations
+    neuralNetworks.f90:45-49,69-80)."""
     import indep_torch as T
 
     if case == "example":
         m, s = ex_model, c1[0]
-    else:
+    elif case == "small_cell":
         m, s = abx3_model, small_cell(W, seed=11)
+    else:
+        m, s = prz_model, small_cell(W, seed=12)
     desc = T.describe(m)
     E, F, dl = T.energy_forces_dEdLat(desc, s["Z"], s["pos"], s["lat"])
     r = m.eval(s["Z"], s["pos"], s["lat"])
@@ -146,9 +151,10 @@ def test_grid_vs_brute_neighbours(case, ex_model, abx3_model, c1, W):
     assert (a[1][:, 0] == np.arange(len(s["Z"]))).all()
 
 
-@pytest.mark.parametrize("case", ["example", "small_cell"])
-def test_fused_vs_single_sf(case, ex_model, abx3_model, c1, W):
-    m, s = (ex_model, c1[0]) if case == "example" else (abx3_model, small_cell(W))
+@pytest.mark.parametrize("case", ["example", "small_cell", "prz_cell"])
+def test_fused_vs_single_sf(case, ex_model, abx3_model, prz_model, c1, W):
+    m, s = {"example": (ex_model, c1[0]), "small_cell": (abx3_model, small_cell(W)),
+            "prz_cell": (prz_model, small_cell(W, seed=13))}[case]
     cap = int(m.neighbours(s["Z"], s["pos"], s["lat"])[0].max())
     G1, d1 = m.symfunctions(s["Z"], s["pos"], s["lat"], with_grad=True, cap=cap)
     G2, d2 = m.symfunctions(s["Z"], s["pos"], s["lat"], separate=True, with_grad=True, cap=cap)
