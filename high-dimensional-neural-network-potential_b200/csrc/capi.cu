@@ -198,6 +198,17 @@ struct hdnnp_ctx {
     DevBuf<int> cnei_cnt, cnei_off, cnei_j, cnei_s, cnei_rev, cnei_map;  // compacted Verlet-skin lists
     DevBuf<int> pad;                                      // padded neighbour rows (int2 pairs)
     int m_est = 0;  // largest neighbour count counted on the host by hdnnp_eval_batch (0: none yet)
+    bool last_fast = false, last_mixed = false;  // kernel family and precision of the last lists stage
+    int stage_seq = 0;  // stage API: 1 after hdnnp_calc_neighbor_lists, 2 after hdnnp_calc_symfunctions
+    int stage_periodic = 0;
+    // One molecule of at most kSmallMolecule atoms per call in FP64: the
+    // single-block kernel of fused_md.cu in evaluation mode (option
+    // "small_eval", default on).  se_dev: the io block (see small_eval_io)
+    // and the kernel's global homes; se_host: its pinned mirror.
+    int small_eval = 1;
+    void* se_dev = nullptr;
+    unsigned char* se_host = nullptr;
+    Batch se_b{};
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
     bool prof_pending = false;
@@ -226,6 +237,8 @@ struct hdnnp_ctx {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
+        if (se_dev) cudaFree(se_dev);
+        if (se_host) cudaFreeHost(se_host);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -526,6 +539,8 @@ int upload_model(hdnnp_model* m) {
     return HDNNP_OK;
 }
 
+bool h_status_ok(const hdnnp_ctx* c) { return c->h_status != nullptr; }
+
 int check_status(hdnnp_ctx* c) {
     int f = c->h_status[0];
     if (f & 1) return fail(HDNNP_E_INPUT, "atom with an element that is not in the potential");
@@ -551,16 +566,52 @@ int collect_profile(hdnnp_ctx* c) {
 
 // Core pipeline; inputs already on the device in c->Z / c->pos (or external
 // device pointers), structure set-up in c->hinfo.
+// Stages of one evaluation, as the reference splits hdnnpEnergyAndForces
+// (hdnnps.f90:346-368): neighbour lists (with the wrap and the element
+// groups), symmetry-function values, and the networks with the force and
+// dE/dh contraction.  A call may run a suffix of them on the lists (and
+// values) the previous call left in the context.
+enum StageBits { kStageLists = 1, kStageSF = 2, kStageNN = 4, kStageAll = 7 };
+
 int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const double* posd, double* energy_d,
                  double* force_d, double* dEdLat_d, cudaStream_t st, PipePlan* pp = nullptr,
-                 const Committee* cm = nullptr) {
+                 const Committee* cm = nullptr, int stages = kStageAll, const DevModel* nn_model = nullptr) {
     hdnnp_model* m = c->model;
     DevModel D = m->dev;
     // runtime-zeta variant of a compiled-zeta shape (same product layout)
     if (c->runtime_zeta && D.fast == 5) D.fast = 1;
     if (c->runtime_zeta && D.fast == 6) D.fast = 2;
-    int ncells = 0;
     int r;
+    if (stages & kStageLists) c->stage_seq = 0;  // the stage API's lists are replaced
+    // stage events only when a call runs the whole evaluation
+    const bool prof = c->profile && stages == kStageAll;
+    int L = 0;
+    Batch b{};
+    bool fast = false, mixed = false;
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (pp) CUDA_TRY(cudaStreamIsCapturing(st, &capturing));
+    auto mark = [&](int k) -> int {
+        if (!prof) return HDNNP_OK;
+        // inside a stream capture only an external record becomes a graph node
+        if (capturing == cudaStreamCaptureStatusActive)
+            CUDA_TRY(cudaEventRecordWithFlags(c->ev[k], st, cudaEventRecordExternal));
+        else
+            CUDA_TRY(cudaEventRecord(c->ev[k], st));
+        return HDNNP_OK;
+    };
+    if (!(stages & kStageLists)) {
+        // later stages on the lists (and values) of the previous call
+        if (!c->have_last) return fail(HDNNP_E_STATE, "no neighbour lists on this context");
+        b = c->last;
+        b.force = force_d;
+        b.energy = energy_d;
+        b.dEdLat = dEdLat_d;
+        fast = c->last_fast;
+        mixed = c->last_mixed;
+        if (!h_status_ok(c)) return fail(HDNNP_E_STATE, "no neighbour lists on this context");
+        CUDA_TRY(cudaMemsetAsync(b.status, 0, sizeof(int), st));
+    } else {
+    int ncells = 0;
     if (!pp || pp->upload) {
         for (auto& S : c->hinfo) {
             S.cell_off = ncells;
@@ -583,7 +634,6 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
         (r = c->gself.ensure(3 * N)) || (r = c->vir.ensure(9 * N)))
         return r;
     if (!c->h_status) CUDA_TRY(cudaMallocHost(&c->h_status, 4 * sizeof(int)));
-    Batch b{};
     b.nstruct = nstruct;
     b.natoms = natoms;
     b.ncells = ncells;
@@ -619,8 +669,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.rebuild = pp ? pp->rebuild : nullptr;
     b.wshift = pp ? pp->wshift : nullptr;
     b.pos_ref = pp ? pp->pos_ref : nullptr;
-    int L = 0;
-    if (c->profile) {
+    if (prof) {
         // a plan collects the stage times of its replays itself (ctx_profile_replay)
         if ((!pp || pp->eager) && (r = collect_profile(c))) return r;
         for (auto& e : c->ev)
@@ -635,17 +684,6 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             c->host_counts[1] += natoms;
         }
     }
-    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
-    if (pp) CUDA_TRY(cudaStreamIsCapturing(st, &capturing));
-    auto mark = [&](int k) -> int {
-        if (!c->profile) return HDNNP_OK;
-        // inside a stream capture only an external record becomes a graph node
-        if (capturing == cudaStreamCaptureStatusActive)
-            CUDA_TRY(cudaEventRecordWithFlags(c->ev[k], st, cudaEventRecordExternal));
-        else
-            CUDA_TRY(cudaEventRecord(c->ev[k], st));
-        return HDNNP_OK;
-    };
     CUDA_TRY(cudaMemsetAsync(b.status, 0, 4 * sizeof(int), st));
     if ((r = mark(0))) return r;
     if (pp && pp->pad_lists && pp->e_cap > 0) {
@@ -701,8 +739,8 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
         return r;
     // mixed precision runs on the fast (lambda x zeta x eta) kernels; potentials
     // outside their shapes evaluate in FP64 with the generic kernels
-    const bool fast = D.fast && !c->generic_sf;
-    const bool mixed = c->precision == HDNNP_PREC_MIXED && fast;
+    fast = D.fast && !c->generic_sf;
+    mixed = c->precision == HDNNP_PREC_MIXED && fast;
     if (fast) {
         if ((r = c->pairs.ensure(N * (size_t)kPairCap)) || (r = c->npairs.ensure(N))) return r;
         b.pairs = c->pairs.p;
@@ -751,22 +789,32 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if ((r = mark(2))) return r;
     L += launch_element_groups(b, D, st);
     if ((r = mark(3))) return r;
-    L += fast ? launch_sf_values_fast(b, D, mixed, st) : launch_sf_values(b, D, st);
-    if ((r = mark(4))) return r;
-    if (cm)
-        L += launch_committee_networks(b, *cm, mixed, !c->mlp_simt, c->cm_acc.p, c->cm_E.p, st);
-    else if (mixed && D.tc_ok && !c->mlp_simt)
-        L += launch_mlp_tc(b, D, st);
-    else
-        L += mixed ? launch_mlp_fp32(b, D, st) : launch_mlp(b, D, st);
-    if ((r = mark(5))) return r;
-    L += fast ? launch_sf_gradients_fast(b, D, mixed, st) : launch_sf_gradients(b, D, st);
-    if ((r = mark(6))) return r;
-    L += mixed ? launch_forces_and_reduce_fp32(b, D, dEdLat_d != nullptr, st)
-               : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
-    if (cm) L += launch_committee_finish(b, *cm, c->cm_E.p, st);  // mean energies (and std)
-    if ((r = mark(7))) return r;
-    if (c->profile && (!pp || pp->eager)) c->prof_pending = true;
+    c->last_fast = fast;
+    c->last_mixed = mixed;
+    }  // lists stage
+    if (stages & kStageSF) {
+        L += fast ? launch_sf_values_fast(b, D, mixed, st) : launch_sf_values(b, D, st);
+        if ((r = mark(4))) return r;
+    }
+    if (stages & kStageNN) {
+        // networks of the context's potential, of another potential with the
+        // same elements and input widths (nn_model), or of a committee
+        const DevModel& M = nn_model ? *nn_model : D;
+        if (cm)
+            L += launch_committee_networks(b, *cm, mixed, !c->mlp_simt, c->cm_acc.p, c->cm_E.p, st);
+        else if (mixed && M.tc_ok && !c->mlp_simt)
+            L += launch_mlp_tc(b, M, st);
+        else
+            L += mixed ? launch_mlp_fp32(b, M, st) : launch_mlp(b, M, st);
+        if ((r = mark(5))) return r;
+        L += fast ? launch_sf_gradients_fast(b, D, mixed, st) : launch_sf_gradients(b, D, st);
+        if ((r = mark(6))) return r;
+        L += mixed ? launch_forces_and_reduce_fp32(b, D, dEdLat_d != nullptr, st)
+                   : launch_forces_and_reduce(b, D, dEdLat_d != nullptr, st);
+        if (cm) L += launch_committee_finish(b, *cm, c->cm_E.p, st);  // mean energies (and std)
+        if ((r = mark(7))) return r;
+    }
+    if (prof && (!pp || pp->eager)) c->prof_pending = true;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c->h_status, b.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     // without the mid-pipeline host read, the structure a non-finite position
@@ -776,6 +824,99 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     c->launches = L;
     c->last = b;
     c->have_last = true;
+    return HDNNP_OK;
+}
+
+// Io block of the small-molecule evaluation (bytes from the start of
+// se_dev, mirrored in se_host): positions, element indices and the status
+// accumulator go in (one copy); the status, energy and forces come out (one
+// copy).  Sized for kSmallMolecule atoms.
+struct SmallEvalIo {
+    static constexpr size_t pos = 0;                                   // double[3 * kSmallMolecule]
+    static constexpr size_t elem = pos + 8 * 3 * kSmallMolecule;       // int[kSmallMolecule]
+    static constexpr size_t acc = elem + 4 * kSmallMolecule;           // int[2]
+    static constexpr size_t energy = acc + 8;                          // double
+    static constexpr size_t force = energy + 8;                        // double[3 * kSmallMolecule]
+    static constexpr size_t info = (force + 8 * 3 * kSmallMolecule + 255) & ~size_t(255);  // StructInfo
+    static constexpr size_t homes = (info + sizeof(StructInfo) + 255) & ~size_t(255);
+    static constexpr size_t in_bytes = energy - pos;   // pos, elem, acc
+    static constexpr size_t out_off = acc;             // acc, energy, force
+};
+
+// Device homes of the single-block kernel for a molecule of up to
+// kSmallMolecule atoms (the per-step arrays its shared memory cannot hold):
+// allocated once per context.
+int small_eval_setup(hdnnp_ctx* c) {
+    if (c->se_dev) return HDNNP_OK;
+    const DevModel& D = c->model->dev;
+    const size_t N = kSmallMolecule, NN = N * N, nsf = (size_t)D.nsf_max;
+    const size_t nd = 2 * N * nsf + 3 * NN + 9 * N, ni = 3 * NN;
+    const size_t bytes = SmallEvalIo::homes + nd * 8 + ni * 4;
+    CUDA_TRY(cudaMalloc(&c->se_dev, bytes));
+    CUDA_TRY(cudaMallocHost(&c->se_host, SmallEvalIo::homes));
+    std::memset(c->se_host, 0, SmallEvalIo::homes);
+    unsigned char* base = (unsigned char*)c->se_dev;
+    double* d = (double*)(base + SmallEvalIo::homes);
+    int* q = (int*)(d + nd);
+    Batch& b = c->se_b;
+    b = Batch{};
+    b.nstruct = 1;
+    b.G = d; d += N * nsf;
+    b.dEdG = d; d += N * nsf;
+    b.gent = d; d += 3 * NN;
+    b.vir = d;
+    b.nei_j = q; q += NN;
+    b.nei_s = q; q += NN;
+    b.nei_rev = q;
+    b.elem = (int*)(base + SmallEvalIo::elem);
+    b.info = (const StructInfo*)(base + SmallEvalIo::info);
+    StructInfo S{};
+    for (int k = 0; k < 9; ++k) S.h[k] = S.hinv[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    S.ngrid[0] = S.ngrid[1] = S.ngrid[2] = 1;
+    CUDA_TRY(cudaMemcpy(base + SmallEvalIo::info, &S, sizeof S, cudaMemcpyHostToDevice));
+    return HDNNP_OK;
+}
+
+// One molecule of nat <= kSmallMolecule atoms in FP64 through the
+// single-block kernel (fused_md.cu, evaluation mode): one host-to-device
+// copy, one kernel, one device-to-host copy, one wait.  Z must be validated.
+int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, double* energy, double* force) {
+    int r;
+    if ((r = small_eval_setup(c))) return r;
+    const DevModel& D = c->model->dev;
+    unsigned char* h = c->se_host;
+    unsigned char* dv = (unsigned char*)c->se_dev;
+    std::memcpy(h + SmallEvalIo::pos, pos, sizeof(double) * 3 * nat);
+    int* he = (int*)(h + SmallEvalIo::elem);
+    for (int i = 0; i < nat; ++i) he[i] = D.z2e[Z[i]];
+    int* hacc = (int*)(h + SmallEvalIo::acc);
+    hacc[0] = hacc[1] = 0;
+    cudaStream_t st = c->stream;
+    CUDA_TRY(cudaMemcpyAsync(dv, h, SmallEvalIo::in_bytes, cudaMemcpyHostToDevice, st));
+    Batch b = c->se_b;
+    b.natoms = nat;
+    b.mmax = nat - 1;
+    b.nentries = nat * nat;
+    SmallMdArgs a{};
+    a.natoms = nat;
+    a.nsteps = 1;
+    a.dt = 0.0;
+    a.pos = (double*)(dv + SmallEvalIo::pos);
+    a.force = (double*)(dv + SmallEvalIo::force);
+    a.energy = (double*)(dv + SmallEvalIo::energy);
+    a.acc = (int*)(dv + SmallEvalIo::acc);
+    a.eval_only = 1;
+    launch_small_md(b, D, a, st);
+    CUDA_TRY(cudaGetLastError());
+    const size_t out = SmallEvalIo::force + sizeof(double) * 3 * nat - SmallEvalIo::out_off;
+    CUDA_TRY(cudaMemcpyAsync(h + SmallEvalIo::out_off, dv + SmallEvalIo::out_off, out, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    c->launches = 1;
+    c->have_last = false;  // the intermediates are not in the context's arrays
+    if (hacc[0] & 8) return fail(HDNNP_E_INPUT, "non-finite position (structure 0)");
+    if (hacc[0]) return fail(HDNNP_E_STATE, "single-block evaluation: device flags " + std::to_string(hacc[0]));
+    std::memcpy(energy, h + SmallEvalIo::energy, sizeof(double));
+    std::memcpy(force, h + SmallEvalIo::force, sizeof(double) * 3 * nat);
     return HDNNP_OK;
 }
 
@@ -840,6 +981,66 @@ int hdnnp_model_info(const hdnnp_model* m, int* nelem, int* Z, int* nsf, double*
     return HDNNP_OK;
 }
 
+int hdnnp_model_flags(const hdnnp_model* m, int* scalesf, int* centersf, double* emin, double* emax,
+                      double* atomenergies) {
+    if (!m) return fail(HDNNP_E_INPUT, "null model");
+    const HostModel& H = m->host;
+    if (scalesf) *scalesf = H.scalesf ? 1 : 0;
+    if (centersf) *centersf = H.centersf ? 1 : 0;
+    if (emin) *emin = H.emin;
+    if (emax) *emax = H.emax;
+    if (atomenergies) {
+        for (int z = 0; z < kMaxZ; ++z) atomenergies[z] = 0.0;
+        for (const auto& e : H.el) atomenergies[e.z - 1] = e.atom_energy;
+    }
+    return HDNNP_OK;
+}
+
+namespace {
+const ElementModel* element_of(const hdnnp_model* m, int Z) {
+    if (!m || Z < 1 || Z > kMaxZ || m->host.z2e[Z] < 0) return nullptr;
+    return &m->host.el[m->host.z2e[Z]];
+}
+}  // namespace
+
+int hdnnp_model_symfunctions(const hdnnp_model* m, int Z, int* nsf, double* params) {
+    const ElementModel* e = element_of(m, Z);
+    if (!e || !nsf) return fail(HDNNP_E_INPUT, "null argument or element not in the potential");
+    *nsf = (int)e->sfs.size();
+    if (params)
+        for (size_t s = 0; s < e->sfs.size(); ++s) {
+            const SymFn& f = e->sfs[s];
+            const double row[11] = {(double)f.type, (double)f.z1, (double)f.z2, f.rcut, f.eta, f.lambda,
+                                    f.zeta, f.rs, f.smin, f.smax, f.smean};
+            std::memcpy(params + 11 * s, row, sizeof row);
+        }
+    return HDNNP_OK;
+}
+
+int hdnnp_model_network(const hdnnp_model* m, int Z, int* nlayers, int* dims, char* acts, double* values) {
+    const ElementModel* e = element_of(m, Z);
+    if (!e || !nlayers) return fail(HDNNP_E_INPUT, "null argument or element not in the potential");
+    *nlayers = (int)e->net.size();
+    size_t o = 0;
+    for (size_t l = 0; l < e->net.size(); ++l) {
+        const Layer& ly = e->net[l];
+        if (dims) {
+            dims[2 * l] = ly.nin;
+            dims[2 * l + 1] = ly.nout;
+        }
+        if (acts) acts[l] = ly.act;
+        if (values) {
+            // weights(nOut, nInp) column-major, as nnLayer%weights, then bias(nOut)
+            for (int i = 0; i < ly.nin; ++i)
+                for (int k = 0; k < ly.nout; ++k) values[o + (size_t)i * ly.nout + k] = ly.w[(size_t)k * ly.nin + i];
+            o += (size_t)ly.nin * ly.nout;
+            for (int k = 0; k < ly.nout; ++k) values[o + k] = ly.b[k];
+            o += ly.nout;
+        }
+    }
+    return HDNNP_OK;
+}
+
 void hdnnp_model_free(hdnnp_model* m) {
     if (!m) return;
     if (m->dmem) {
@@ -900,6 +1101,10 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
         c->sf_blocks_per_sm = value;
         return HDNNP_OK;
     }
+    if (std::string(name) == "small_eval") {
+        c->small_eval = value != 0;
+        return HDNNP_OK;
+    }
     if (std::string(name) == "nei_warp") {
         if (value < -1 || value > 1) return fail(HDNNP_E_INPUT, "nei_warp must be -1, 0 or 1");
         c->nei_warp = value;
@@ -921,6 +1126,14 @@ int hdnnp_eval_batch(hdnnp_ctx* c, int nstruct, const int64_t* atom_off, const i
     const int natoms = (int)atom_off[nstruct];
     const size_t N = natoms;
     cudaStream_t st = c->stream;
+    // one small molecule in FP64 (the reference's MD example): one kernel
+    if (nstruct == 1 && !(periodic && periodic[0]) && natoms <= kSmallMolecule && c->small_eval &&
+        c->precision == HDNNP_PREC_FP64 && !c->profile &&
+        small_md_smem_bytes(c->model->dev, natoms) <= 226 * 1024) {
+        c->stage_seq = 0;
+        if (dEdLat) std::memset(dEdLat, 0, 9 * sizeof(double));
+        return small_eval(c, natoms, Z, pos, energy, force);
+    }
     if ((r = c->Z.ensure(N)) || (r = c->pos.ensure(3 * N)) || (r = c->force.ensure(3 * N)) ||
         (r = c->energy.ensure(nstruct)) || (r = c->dEdLat.ensure(9 * (size_t)nstruct)))
         return r;
@@ -987,6 +1200,156 @@ int hdnnp_energy_and_forces(hdnnp_ctx* c, int nat, const int32_t* Z, const doubl
     int32_t per = periodic ? 1 : 0;
     double dummy[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     return hdnnp_eval_batch(c, 1, off, Z, pos, &per, lat ? lat : dummy, energy, force, dEdLat);
+}
+
+// ---------------------------------------------------------------- stages
+// hdnnpCalcNeighborLists (hdnnps.f90:373-388): wrap, cell lists and the
+// neighbour lists of one structure, kept in the context.
+int hdnnp_calc_neighbor_lists(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, int periodic,
+                              const double* lat, int* nentries) {
+    if (!c || nat <= 0 || !Z || !pos) return fail(HDNNP_E_INPUT, "null argument or no atoms");
+    if (periodic && !lat) return fail(HDNNP_E_INPUT, "periodic structure without a lattice");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    c->stage_seq = 0;
+    int64_t off[2] = {0, nat};
+    int32_t per = periodic ? 1 : 0;
+    const double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    int r = prepare_structs(c, 1, off, Z, pos, &per, periodic ? lat : ident, true);
+    if (r) return r;
+    const size_t N = nat;
+    cudaStream_t st = c->stream;
+    if ((r = c->Z.ensure(N)) || (r = c->pos.ensure(3 * N)) || (r = c->force.ensure(3 * N)) ||
+        (r = c->energy.ensure(1)) || (r = c->dEdLat.ensure(9)))
+        return r;
+    CUDA_TRY(cudaMemcpyAsync(c->Z.p, Z, sizeof(int32_t) * N, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->pos.p, pos, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    r = run_pipeline(c, 1, nat, c->Z.p, c->pos.p, c->energy.p, c->force.p, c->dEdLat.p, st, nullptr, nullptr,
+                     kStageLists);
+    if (r) return r;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if ((r = check_status(c))) return r;
+    if (nentries) *nentries = c->h_status[2];
+    c->stage_seq = 1;
+    c->stage_periodic = periodic ? 1 : 0;
+    return HDNNP_OK;
+}
+
+// The lists of the last hdnnp_calc_neighbor_lists in the reference's
+// neighborList layout (neighborLists.f90:10-16): per atom nNeis = count + 1
+// entries, entry 1 the atom itself at its wrapped position, then its
+// neighbours (index, Cartesian image position) in list order.
+int hdnnp_neighbor_lists_fetch(hdnnp_ctx* c, int* nneis, int* ineis, double* neis) {
+    if (!c || !nneis) return fail(HDNNP_E_INPUT, "null argument");
+    if (c->stage_seq < 1) return fail(HDNNP_E_STATE, "no lists: call hdnnp_calc_neighbor_lists first");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    const Batch& b = c->last;
+    const int nat = b.natoms;
+    std::vector<int> cnt(nat), off(nat + 1);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpy(cnt.data(), b.nei_cnt, sizeof(int) * nat, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(off.data(), b.nei_off, sizeof(int) * (nat + 1), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nat; ++i) nneis[i] = cnt[i] + 1;
+    if (!ineis && !neis) return HDNNP_OK;
+    const size_t E = (size_t)off[nat];
+    std::vector<int> nj(E), ns(E);
+    std::vector<double> w(3 * (size_t)nat);
+    if (E) {
+        CUDA_TRY(cudaMemcpy(nj.data(), b.nei_j, sizeof(int) * E, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(ns.data(), b.nei_s, sizeof(int) * E, cudaMemcpyDeviceToHost));
+    }
+    CUDA_TRY(cudaMemcpy(w.data(), b.wpos, sizeof(double) * 3 * nat, cudaMemcpyDeviceToHost));
+    const StructInfo& S = c->hinfo[0];
+    size_t o = 0;
+    for (int i = 0; i < nat; ++i) {
+        if (ineis) ineis[o] = i;
+        if (neis)
+            for (int d = 0; d < 3; ++d) neis[3 * o + d] = w[3 * (size_t)i + d];
+        ++o;
+        for (int q = off[i]; q < off[i + 1]; ++q, ++o) {
+            const int j = nj[q];
+            if (ineis) ineis[o] = j;
+            if (!neis) continue;
+            int sx, sy, sz;
+            unpack_shift(ns[q], sx, sy, sz);
+            // image shift summed z, y, x as in the neighbour search
+            double l[3] = {0.0, 0.0, 0.0};
+            for (int d = 0; d < 3; ++d) {
+                if (sz) l[d] += S.h[6 + d] * sz;
+                if (sy) l[d] += S.h[3 + d] * sy;
+                if (sx) l[d] += S.h[0 + d] * sx;
+            }
+            for (int d = 0; d < 3; ++d) neis[3 * o + d] = w[3 * (size_t)j + d] + l[d];
+        }
+    }
+    return HDNNP_OK;
+}
+
+// hdnnpCalcSymfunctions (hdnnps.f90:390-485): the scaled symmetry-function
+// values of the structure whose lists the context holds; G (host, nat x
+// nsf_max, row stride nsf_max, unused columns of elements with fewer
+// functions are zero) may be NULL.  Derivatives are not stored: the
+// contraction recomputes them (hdnnp_calc_nns).
+int hdnnp_calc_symfunctions(hdnnp_ctx* c, double* G) {
+    if (!c) return fail(HDNNP_E_INPUT, "null context");
+    if (c->stage_seq < 1) return fail(HDNNP_E_STATE, "hdnnp_calc_symfunctions needs hdnnp_calc_neighbor_lists first");
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    const int nat = c->last.natoms;
+    cudaStream_t st = c->stream;
+    int r = run_pipeline(c, 1, nat, c->Z.p, c->pos.p, c->energy.p, c->force.p, nullptr, st, nullptr, nullptr,
+                         kStageSF);
+    if (r) return r;
+    c->last.dEdLat = nullptr;
+    const size_t n = (size_t)nat * c->model->dev.nsf_max;
+    std::vector<float> tmp;
+    if (G) {
+        if (c->last_mixed) {
+            tmp.resize(n);
+            CUDA_TRY(cudaMemcpyAsync(tmp.data(), c->last.Gf, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        } else {
+            CUDA_TRY(cudaMemcpyAsync(G, c->last.G, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if ((r = check_status(c))) return r;
+    if (G && c->last_mixed)
+        for (size_t q = 0; q < n; ++q) G[q] = (double)tmp[q];
+    c->stage_seq = 2;
+    return HDNNP_OK;
+}
+
+// hdnnpCalcNNs (hdnnps.f90:487-562): the networks of `nn` (NULL: the
+// context's potential) on the symmetry functions the context holds, and the
+// contraction into energy, forces and (periodic structures) dE/dh.  As in the
+// reference's committee (globalHdnnps.f90:47-57) the functions and their
+// derivatives are those of the context's potential, and `nn` must have the
+// same elements and network input widths.  May be called repeatedly.
+int hdnnp_calc_nns(hdnnp_ctx* c, const hdnnp_model* nn, double* energy, double* force, double* dEdLat) {
+    if (!c || !energy || !force) return fail(HDNNP_E_INPUT, "null argument");
+    if (c->stage_seq < 2) return fail(HDNNP_E_STATE, "hdnnp_calc_nns needs hdnnp_calc_symfunctions first");
+    if (dEdLat && !c->stage_periodic) return fail(HDNNP_E_INPUT, "dEdLat needs a periodic structure");
+    const HostModel& H0 = c->model->host;
+    if (nn && nn != c->model) {
+        if (nn->device != c->model->device) return fail(HDNNP_E_INPUT, "the network's potential lives on another device");
+        const HostModel& Hq = nn->host;
+        if (Hq.el.size() != H0.el.size()) return fail(HDNNP_E_INPUT, "the network's potential has other elements");
+        for (size_t e = 0; e < H0.el.size(); ++e)
+            if (Hq.el[e].z != H0.el[e].z || Hq.el[e].net.empty() || Hq.el[e].net[0].nin != (int)H0.el[e].sfs.size())
+                return fail(HDNNP_E_INPUT, "the network's potential: elements or network input widths differ from the "
+                                           "symmetry functions of the context's potential");
+        const size_t tc = mlp_smem_bytes(nn->dev, c->last_mixed ? sizeof(float) : sizeof(double));
+        if (tc > 220 * 1024) return fail(HDNNP_E_CAPACITY, "network too wide for the MLP kernel");
+    }
+    CUDA_TRY(cudaSetDevice(c->model->device));
+    const int nat = c->last.natoms;
+    cudaStream_t st = c->stream;
+    int r = run_pipeline(c, 1, nat, c->Z.p, c->pos.p, c->energy.p, c->force.p, dEdLat ? c->dEdLat.p : nullptr, st,
+                         nullptr, nullptr, kStageNN, (nn && nn != c->model) ? &nn->dev : nullptr);
+    if (r) return r;
+    CUDA_TRY(cudaMemcpyAsync(energy, c->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(force, c->force.p, sizeof(double) * 3 * (size_t)nat, cudaMemcpyDeviceToHost, st));
+    if (dEdLat) CUDA_TRY(cudaMemcpyAsync(dEdLat, c->dEdLat.p, sizeof(double) * 9, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return check_status(c);
 }
 
 int hdnnp_committee_eval_batch(hdnnp_ctx* c, hdnnp_model* const* members, int nmembers, int nstruct,

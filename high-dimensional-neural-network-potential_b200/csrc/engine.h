@@ -246,6 +246,7 @@ struct SmallMdArgs {
     double* energy;
     double* hist;       // [nsteps] energies or null
     int* acc;           // [2]: OR of status flags, evaluations
+    int eval_only;      // 1: one evaluation of pos (nsteps 1), no MD; mom and mass unused
 };
 
 // packed image shift: three signed 8-bit lattice multiples

@@ -49,6 +49,7 @@ struct FusedArgs {
     double* energy;
     double* hist;                        // [nsteps] or null
     int* acc;                            // [2]: OR of status flags, evaluations
+    int eval_only;                       // 1: one evaluation of pos, no MD (mom, mass unused)
 };
 
 template <typename P>
@@ -159,11 +160,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_small_md(Batch g, DevModel m, F
     b.stats = nullptr;
     for (int q = tid; q < n3; q += blockDim.x) {
         pos[q] = a.pos[q];
-        mom[q] = a.mom[q];
-        F[q] = a.force[q];
+        mom[q] = a.eval_only ? 0.0 : a.mom[q];
+        F[q] = a.eval_only ? 0.0 : a.force[q];
     }
     for (int i = tid; i < N; i += blockDim.x) {
-        mass[i] = a.mass[i];
+        mass[i] = a.eval_only ? 1.0 : a.mass[i];
         b.elem[i] = g.elem[i];
         b.sid[i] = 0;
     }
@@ -175,6 +176,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_small_md(Batch g, DevModel m, F
         // kick of the previous step and drift (hdnnpExample.f90:61-64),
         // element by element in the same thread
         for (int q = tid; q < n3; q += blockDim.x) {
+            if (a.eval_only) {  // positions as given
+                if (!isfinite(pos[q])) atomicOr(b.status, 8);
+                continue;
+            }
             const double mi = mass[q / 3];
             double p = mom[q];
             if (step > 0) p += 0.5 * dt * (F[q] + Fp[q]);
@@ -274,8 +279,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_small_md(Batch g, DevModel m, F
     }
     // last kick; the state back to the plan's arrays
     for (int q = tid; q < n3; q += blockDim.x) {
-        a.mom[q] = mom[q] + 0.5 * dt * (F[q] + Fp[q]);
-        a.pos[q] = pos[q];
+        if (!a.eval_only) {
+            a.mom[q] = mom[q] + 0.5 * dt * (F[q] + Fp[q]);
+            a.pos[q] = pos[q];
+        }
         a.force[q] = F[q];
     }
     if (tid == 0) {
@@ -366,6 +373,7 @@ struct TinyArgs {
     double* hist;
     int* acc;
     const int* elem;
+    int eval_only;                  // 1: one evaluation of pos, no MD (mom, mass unused)
 };
 
 // pair r of one centre's list (0 <= p < q): r = q (q - 1) / 2 + p
@@ -426,11 +434,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
     int* status = (int*)(smem + a.slot[tStatus]);
     for (int q = tid; q < n3; q += nt) {
         pos[q] = a.pos[q];
-        mom[q] = a.mom[q];
-        F[q] = a.force[q];
+        mom[q] = a.eval_only ? 0.0 : a.mom[q];
+        F[q] = a.eval_only ? 0.0 : a.force[q];
     }
     for (int i = tid; i < N; i += nt) {
-        mass[i] = a.mass[i];
+        mass[i] = a.eval_only ? 1.0 : a.mass[i];
         elem[i] = a.elem[i];
     }
     for (int x = tid; x < nel * nblk; x += nt)
@@ -444,6 +452,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
     for (int step = 0; step < a.nsteps; ++step) {
         // kick of the previous step and drift (hdnnpExample.f90:61-64)
         for (int q = tid; q < n3; q += nt) {
+            if (a.eval_only) {  // positions as given
+                if (!isfinite(pos[q])) atomicOr(status, 8);
+                continue;
+            }
             const double mi = mass[q / 3];
             double p = mom[q];
             if (step > 0) p += 0.5 * dt * (F[q] + Fp[q]);
@@ -771,8 +783,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
         __syncthreads();
     }
     for (int q = tid; q < n3; q += nt) {
-        a.mom[q] = mom[q] + 0.5 * dt * (F[q] + Fp[q]);
-        a.pos[q] = pos[q];
+        if (!a.eval_only) {
+            a.mom[q] = mom[q] + 0.5 * dt * (F[q] + Fp[q]);
+            a.pos[q] = pos[q];
+        }
         a.force[q] = F[q];
     }
     if (tid == 0) {
@@ -838,6 +852,7 @@ int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& x, cud
         ta.hist = x.hist;
         ta.acc = x.acc;
         ta.elem = b.elem;
+        ta.eval_only = x.eval_only;
         cudaFuncSetAttribute(k_tiny_md, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
         k_tiny_md<<<1, kThreads, tsm, s>>>(m, ta);
         return 1;
@@ -855,6 +870,7 @@ int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& x, cud
     a.energy = x.energy;
     a.hist = x.hist;
     a.acc = x.acc;
+    a.eval_only = x.eval_only;
     auto run = [&](auto kernel) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kernel<<<1, kThreads, smem, s>>>(b, m, a);

@@ -14,6 +14,14 @@ dEdLat2Stress(lat, dEdLat, s)  ``dEdLat_to_stress`` (atomicStructure.f90:679)
 globalHdnnpEnergyAndForces(    ``h.committee_energy_and_forces(members, ats)``
   ats, energy, forces,          -> (energy, forces, dEdLat, std)
   dEdLat, std)                  (globalHdnnps.f90:31)
+hdnnpCalcNeighborLists(h, ats, ``h.calc_neighbor_lists(ats)``        (:373)
+  neiLists)
+hdnnpCalcSymfunctions(h, ats,  ``h.calc_symfunctions()`` -> G        (:390)
+  neiLists, sfs)
+hdnnpCalcNNs(h, ats, neiLists, ``h.calc_nns(nn=None, dEdLat=False)`` (:487)
+  sfs, energy, force, dEdLat)
+handle%sfLists / nnList /      ``h.symfunctions(z)``, ``h.network(z)``,
+  scalesf / centersf / ...      ``h.flags()``                      (:13-21)
 =============================  ==============================================
 
 Errors that make the reference ``stop`` raise ``HdnnpError`` here.  Arrays
@@ -78,6 +86,13 @@ def lib():
     L.hdnnp_profile_read.argtypes = [P, D, I64, C.c_int]
     L.hdnnp_committee_energy_and_forces.argtypes = [P, P, C.c_int, C.c_int, I, D, C.c_int, D, D, D, D, D]
     L.hdnnp_committee_eval_batch.argtypes = [P, P, C.c_int, C.c_int, I64, I, D, I, D, D, D, D, D]
+    L.hdnnp_calc_neighbor_lists.argtypes = [P, C.c_int, I, D, C.c_int, D, C.POINTER(C.c_int)]
+    L.hdnnp_calc_symfunctions.argtypes = [P, D]
+    L.hdnnp_neighbor_lists_fetch.argtypes = [P, I, I, D]
+    L.hdnnp_calc_nns.argtypes = [P, P, D, D, D]
+    L.hdnnp_model_flags.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), D, D, D]
+    L.hdnnp_model_symfunctions.argtypes = [P, C.c_int, C.POINTER(C.c_int), D]
+    L.hdnnp_model_network.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p, D]
     L.hdnnp_server_create.argtypes = [P, P, C.POINTER(C.c_void_p)]
     L.hdnnp_server_destroy.argtypes = [P]
     L.hdnnp_server_destroy.restype = None
@@ -203,6 +218,87 @@ class Hdnnp:
         lat = np.concatenate([_lat_flat(s["lat"]) for s in structs])
         per = np.array([0 if s["lat"] is None else 1 for s in structs], np.int32)
         return self.eval_batch_arrays(off, Z, pos, per, lat, dEdLat)
+
+    # ------------------------------------------------------------------ stages
+    def calc_neighbor_lists(self, ats: AtStruct) -> int:
+        """hdnnpCalcNeighborLists (hdnnps.f90:373): the lists stay on the
+        device in this potential's context; returns the neighbour entries."""
+        n = C.c_int()
+        _check(lib().hdnnp_calc_neighbor_lists(self._c, ats.nat, _ip(ats.el), _dp(ats.ats), 1 if ats.periodic else 0,
+                                               _dp(_lat_flat(ats.lat)), C.byref(n)))
+        self._stage_nat = ats.nat
+        return n.value
+
+    def neighbor_lists(self):
+        """The lists of the last calc_neighbor_lists as the reference's
+        neighborList (neighborLists.f90:10-16): per atom (iNeis, neis(nNei,
+        3)), entry 0 the atom itself, 0-based indices."""
+        n = np.zeros(self._stage_nat, np.int32)
+        _check(lib().hdnnp_neighbor_lists_fetch(self._c, _ip(n), None, None))
+        tot = int(n.sum())
+        idx = np.zeros(tot, np.int32)
+        pos = np.zeros((tot, 3))
+        _check(lib().hdnnp_neighbor_lists_fetch(self._c, _ip(n), _ip(idx), _dp(pos)))
+        off = np.concatenate([[0], np.cumsum(n)])
+        return [(idx[off[i]:off[i + 1]], pos[off[i]:off[i + 1]]) for i in range(len(n))]
+
+    def calc_symfunctions(self, fetch: bool = True):
+        """hdnnpCalcSymfunctions (hdnnps.f90:390): scaled G of the structure
+        of the last calc_neighbor_lists, (nat, nsf_max) when ``fetch``."""
+        G = np.zeros((self._stage_nat, max(self.nsf.values()))) if fetch else None
+        _check(lib().hdnnp_calc_symfunctions(self._c, _dp(G)))
+        return G
+
+    def calc_nns(self, nn: Optional["Hdnnp"] = None, dEdLat: bool = False):
+        """hdnnpCalcNNs (hdnnps.f90:487): the networks of ``nn`` (default:
+        this potential) on this context's symmetry functions; energy, forces
+        (nat, 3) and dE/dh (3, 3) or None."""
+        E = C.c_double()
+        F = np.zeros((self._stage_nat, 3))
+        dl = np.zeros(9) if dEdLat else None
+        _check(lib().hdnnp_calc_nns(self._c, None if nn is None else nn._m, C.byref(E), _dp(F), _dp(dl)))
+        return E.value, F, (dl.reshape(3, 3, order="F") if dl is not None else None)
+
+    # ------------------------------------------------------------------ type(hdnnp) components
+    def flags(self):
+        """scalesf, centersf, emin, emax and atomenergies(118) (hdnnps.f90:13-21)."""
+        sc, ce = C.c_int(), C.c_int()
+        emin, emax = C.c_double(), C.c_double()
+        ae = np.zeros(118)
+        _check(lib().hdnnp_model_flags(self._m, C.byref(sc), C.byref(ce), C.byref(emin), C.byref(emax), _dp(ae)))
+        return {"scalesf": bool(sc.value), "centersf": bool(ce.value), "emin": emin.value, "emax": emax.value,
+                "atomenergies": ae}
+
+    def symfunctions(self, z: int) -> np.ndarray:
+        """sfLists(z): (nsf, 11) rows name, el1, el2, rcut, eta, lambda, zeta,
+        Rs, sfmin, sfmax, sfmean in the reference's sorted order."""
+        n = C.c_int()
+        _check(lib().hdnnp_model_symfunctions(self._m, int(z), C.byref(n), None))
+        out = np.zeros((n.value, 11))
+        _check(lib().hdnnp_model_symfunctions(self._m, int(z), C.byref(n), _dp(out)))
+        return out
+
+    def network(self, z: int):
+        """nnList(z): [(W (nout, nin), b (nout,), activation), ...]."""
+        nl = C.c_int()
+        _check(lib().hdnnp_model_network(self._m, int(z), C.byref(nl), None, None, None))
+        dims = np.zeros(2 * nl.value, np.int32)
+        acts = C.create_string_buffer(nl.value + 1)
+        _check(lib().hdnnp_model_network(self._m, int(z), C.byref(nl), dims.ctypes.data_as(C.POINTER(C.c_int)),
+                                         acts, None))
+        total = sum(int(dims[2 * l]) * int(dims[2 * l + 1]) + int(dims[2 * l + 1]) for l in range(nl.value))
+        vals = np.zeros(total)
+        _check(lib().hdnnp_model_network(self._m, int(z), C.byref(nl), dims.ctypes.data_as(C.POINTER(C.c_int)),
+                                         acts, _dp(vals)))
+        out, o = [], 0
+        for l in range(nl.value):
+            nin, nout = int(dims[2 * l]), int(dims[2 * l + 1])
+            W = vals[o:o + nin * nout].reshape(nin, nout).T.copy()  # Fortran (nout, nin) order
+            o += nin * nout
+            b = vals[o:o + nout].copy()
+            o += nout
+            out.append((W, b, acts.raw[l:l + 1].decode()))
+        return out
 
     # ------------------------------------------------------------------ committee
     def committee_energy_and_forces(self, members: Sequence["Hdnnp"], ats: AtStruct, dEdLat: bool = False):

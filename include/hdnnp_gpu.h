@@ -68,6 +68,26 @@ int hdnnp_model_load_runner(const char* path, int device, hdnnp_model** out);
  * length >= 118.  max_rc = largest cutoff (hdnnp%maxRc, hdnnps.f90:16).    */
 int hdnnp_model_info(const hdnnp_model* m, int* nelem, int* Z, int* nsf, double* max_rc);
 
+/* The components of type(hdnnp) (hdnnps.f90:13-21) as parsed, for callers
+ * that read them: scalesf, centersf, emin, emax (read by readScaling,
+ * :269-300, and unused by the prediction) and atomenergies(118), indexed by
+ * atomic number - 1 (0 for elements not in the potential); each may be NULL. */
+int hdnnp_model_flags(const hdnnp_model* m, int* scalesf, int* centersf, double* emin, double* emax,
+                      double* atomenergies);
+
+/* sfLists(Z) (type symFunctionList, symmetryFunctions.f90:18-21) in the
+ * reference's sorted order: nsf and, if params != NULL, 11 doubles per
+ * function: name (2 or 3), sfEls(1), sfEls(2) (atomic numbers; 0 for type 2),
+ * rcut, eta, lambda, zeta, Rs, sfmin, sfmax, sfmean.  HDNNP_E_INPUT if Z is
+ * not an element of the potential.                                          */
+int hdnnp_model_symfunctions(const hdnnp_model* m, int Z, int* nsf, double* params);
+
+/* nnList(Z) (type neuralNetwork, neuralNetworks.f90:24-28): nlayers and, when
+ * non-NULL, dims[2*l] = nInp and dims[2*l+1] = nOut of layer l, acts[l] its
+ * activation ('l', 't', 'p', 'r'), and values = for each layer
+ * weights(nOut, nInp) in Fortran (column-major) order, then bias(nOut).     */
+int hdnnp_model_network(const hdnnp_model* m, int Z, int* nlayers, int* dims, char* acts, double* values);
+
 void hdnnp_model_free(hdnnp_model* m);
 
 /* ---------------------------------------------------------------- context
@@ -87,7 +107,13 @@ int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
  * kernel with that zeta set compiled in exists.  Results agree within
  * rounding.  "nei_warp" chooses how neighbour lists are built: 1 one warp per
  * atom, -1 one thread per atom, 0 (default) a warp per atom below 131,072
- * atoms in the batch; both give the same lists, entry for entry.             */
+ * atoms in the batch; both give the same lists, entry for entry.
+ * "small_eval" (default 1): a call of one molecule of at most 64 atoms in
+ * FP64 (the reference's own MD example is one) runs as one kernel launch, a
+ * thread block that builds the lists by direct search and keeps every
+ * intermediate on chip, between one copy in and one copy out; 0 runs it
+ * through the general pipeline (same results within rounding; the
+ * intermediates of hdnnp_debug_fetch exist only then).                      */
 int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
 
 /* ---------------------------------------------------------------- evaluation
@@ -99,6 +125,48 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
  * reference reads an uninitialised lattice otherwise, hdnnps.f90:509).     */
 int hdnnp_energy_and_forces(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, int periodic,
                             const double* lat, double* energy, double* force, double* dEdLat);
+
+/* The three stages of hdnnp_energy_and_forces as separate calls, as the
+ * reference makes them public for its committee (globalHdnnps.f90:47-57).
+ * Lists and values stay in the context's device memory between the calls
+ * (the reference hands neiLists and sfs back to the caller).
+ *
+ * hdnnpCalcNeighborLists (hdnnps.f90:373-388): wraps the structure, builds
+ * its neighbour lists and keeps them in `c`; nentries (may be NULL) receives
+ * the number of neighbour entries, not counting the atoms themselves (the
+ * reference stores each atom as entry 1 of its own list).                   */
+int hdnnp_calc_neighbor_lists(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, int periodic,
+                              const double* lat, int* nentries);
+
+/* The lists of the last hdnnp_calc_neighbor_lists on `c` in the layout of
+ * the reference's type neighborList (neighborLists.f90:10-16): nneis[nat]
+ * entries per atom (count + 1); if non-NULL, ineis[sum nneis] the 0-based
+ * atom index of each entry and neis[3 * sum nneis] its Cartesian position
+ * (image of the wrapped position), atom by atom, entry 1 of each atom being
+ * the atom itself.  Size ineis and neis from nneis (a first call with both
+ * NULL).                                                                     */
+int hdnnp_neighbor_lists_fetch(hdnnp_ctx* c, int* nneis, int* ineis, double* neis);
+
+/* hdnnpCalcSymfunctions (hdnnps.f90:390-485): the centred and scaled
+ * symmetry functions of the structure of the last hdnnp_calc_neighbor_lists
+ * on `c`.  G (may be NULL) receives them on the host, nat x nsf_max with row
+ * stride nsf_max (nsf_max = the largest symmetry-function count of the
+ * potential; unused columns are zero).  Their derivatives are not stored:
+ * hdnnp_calc_nns recomputes them in its contraction, where the reference
+ * keeps dsf(3, nNei) for every function and atom.  HDNNP_E_STATE without
+ * lists.                                                                     */
+int hdnnp_calc_symfunctions(hdnnp_ctx* c, double* G);
+
+/* hdnnpCalcNNs (hdnnps.f90:487-562): the networks of `nn` (NULL: the
+ * potential of `c`) on the symmetry functions of the last
+ * hdnnp_calc_symfunctions on `c`, and the contraction into energy, forces and
+ * dEdLat (NULL, or a periodic structure).  `nn` must have the elements and
+ * network input widths of the potential of `c`, whose symmetry functions and
+ * derivatives are used (as globalHdnnpEnergyAndForces does, :51-57).  May be
+ * called several times on the same values.  HDNNP_E_STATE without values.
+ * The chain of the three calls gives bitwise the results of
+ * hdnnp_energy_and_forces.                                                   */
+int hdnnp_calc_nns(hdnnp_ctx* c, const hdnnp_model* nn, double* energy, double* force, double* dEdLat);
 
 /* Batch of nstruct independent structures in CSR form (no reference
  * counterpart: the reference evaluates one structure per call).

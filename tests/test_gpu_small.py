@@ -1,0 +1,95 @@
+"""The plain entry point on small molecules: one FP64 molecule of at most 64
+atoms per call (the reference's MD example calls hdnnpEnergyAndForces this
+way, hdnnpExample.f90:58-63) runs as one single-block kernel launch in
+evaluation mode, between one copy in and one copy out.
+
+* Equal to the general pipeline (option small_eval 0) within rounding and to
+  the FP64 oracle within the FP64 tolerances (|dE| <= 1e-10 |E|, max |dF| <=
+  1e-9 Ha/Bohr), for 1 to 64 atoms, both forms of the kernel (item-parallel
+  up to ~14 atoms, warp per atom above);
+* exactly one kernel launch per call; 65 atoms, periodic cells and the mixed
+  precision use the pipeline;
+* non-finite positions and unknown elements are status codes and the context
+  stays usable.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ABX3_DIR, EXAMPLE_DIR
+
+pytestmark = pytest.mark.gpu
+
+E_REL, F_ABS = 1e-10, 1e-9
+
+
+@pytest.fixture(scope="module")
+def eng(pkg):
+    from hdnnp_b200 import engine
+
+    return engine
+
+
+def clusters(W):
+    rng = np.random.default_rng(81)
+    blob = W.supercell(W.abx3_cell(), (2, 2, 2))
+    pos = blob["pos"] + rng.normal(0.0, 0.05, blob["pos"].shape)
+    out = []
+    for n in (1, 2, 5, 13, 31, 60, 64):
+        # the n atoms nearest the centre of the 96-atom block
+        d = np.linalg.norm(pos - pos.mean(axis=0), axis=1)
+        k = np.sort(np.argsort(d)[:n])
+        out.append({"Z": blob["Z"][k], "pos": pos[k], "lat": None})
+    return out
+
+
+def test_small_molecules_single_kernel(eng, W, orc, c1):
+    cases = [(EXAMPLE_DIR, c1[0])] + [(ABX3_DIR, m) for m in clusters(W)]
+    pots = {d: eng.Hdnnp.from_runner(d) for d in (EXAMPLE_DIR, ABX3_DIR)}
+    ref_pots = {d: eng.Hdnnp.from_runner(d) for d in (EXAMPLE_DIR, ABX3_DIR)}
+    try:
+        for p in ref_pots.values():
+            p.set_option("small_eval", 0)
+        for d, s in cases:
+            ats = eng.AtStruct(s["Z"], s["pos"])
+            E, F, _ = pots[d].energy_and_forces(ats)
+            assert pots[d].launches() == 1, len(s["Z"])
+            E0, F0, _ = ref_pots[d].energy_and_forces(ats)
+            assert ref_pots[d].launches() > 1
+            assert abs(E - E0) <= 1e-12 * max(1.0, abs(E0)), (len(s["Z"]), E, E0)
+            assert np.abs(F - F0).max() <= 1e-11, len(s["Z"])
+            ref = orc.Model(d).eval(s["Z"], s["pos"])
+            assert abs(E - ref["energy"]) <= E_REL * abs(ref["energy"])
+            assert np.abs(F - ref["forces"]).max() <= F_ABS
+    finally:
+        for p in list(pots.values()) + list(ref_pots.values()):
+            p.close()
+
+
+def test_small_path_boundaries_and_errors(eng, W, c1):
+    pot = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        blob = W.supercell(W.abx3_cell(), (2, 2, 2))
+        big = {"Z": blob["Z"][:65], "pos": blob["pos"][:65] + 0.01}
+        pot.energy_and_forces(eng.AtStruct(big["Z"], big["pos"]))
+        assert pot.launches() > 1  # 65 atoms: the pipeline
+        cell = W.abx3_cell()
+        pot.energy_and_forces(eng.AtStruct(cell["Z"], cell["pos"], cell["lat"]))
+        assert pot.launches() > 1  # periodic: the pipeline
+        pot.set_precision(eng.HDNNP_PREC_MIXED)
+        pot.energy_and_forces(eng.AtStruct(cell["Z"], cell["pos"]))
+        assert pot.launches() > 1  # mixed precision: the pipeline
+        pot.set_precision(eng.HDNNP_PREC_FP64)
+        mol = {"Z": cell["Z"], "pos": cell["pos"].copy()}
+        mol["pos"][3, 2] = np.inf
+        with pytest.raises(eng.HdnnpError, match="non-finite"):
+            pot.energy_and_forces(eng.AtStruct(mol["Z"], mol["pos"]))
+        Z = cell["Z"].copy()
+        Z[1] = 8
+        with pytest.raises(eng.HdnnpError, match="not in the potential"):
+            pot.energy_and_forces(eng.AtStruct(Z, cell["pos"]))
+        E, F, _ = pot.energy_and_forces(eng.AtStruct(cell["Z"], cell["pos"]))
+        assert np.isfinite(E) and pot.launches() == 1
+    finally:
+        pot.close()
