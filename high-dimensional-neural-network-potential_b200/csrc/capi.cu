@@ -197,6 +197,8 @@ struct hdnnp_ctx {
     DevBuf<int> npairs;
     DevBuf<int> cnei_cnt, cnei_off, cnei_j, cnei_s, cnei_rev, cnei_map;  // compacted Verlet-skin lists
     DevBuf<int> pad;                                      // padded neighbour rows (int2 pairs)
+    DevBuf<double4> posc;                                 // cell-ordered wrapped positions
+    DevBuf<unsigned short> slab;                          // slab prefixes of the padded rows
     int m_est = 0;  // largest neighbour count counted on the host by hdnnp_eval_batch (0: none yet)
     bool last_fast = false, last_mixed = false;  // kernel family and precision of the last lists stage
     int stage_seq = 0;  // stage API: 1 after hdnnp_calc_neighbor_lists, 2 after hdnnp_calc_symfunctions
@@ -234,6 +236,8 @@ struct hdnnp_ctx {
         pairs.release();
         npairs.release();
         for (auto* b : {&cnei_cnt, &cnei_off, &cnei_j, &cnei_s, &cnei_rev, &cnei_map, &pad}) b->release();
+        slab.release();
+        posc.release();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
@@ -627,7 +631,8 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     const size_t N = natoms;
     if ((r = c->sid.ensure(N)) || (r = c->elem.ensure(N)) || (r = c->wpos.ensure(3 * N)) || (r = c->cell_of.ensure(N)) ||
         (r = c->cell_cnt.ensure(ncells + 1)) || (r = c->cell_start.ensure(ncells + 1)) ||
-        (r = c->cell_atoms.ensure(N)) || (r = c->nei_cnt.ensure(N + 1)) || (r = c->nei_off.ensure(N + 1)) ||
+        (r = c->cell_atoms.ensure(N)) || (r = c->posc.ensure(N)) || (r = c->nei_cnt.ensure(N + 1)) ||
+        (r = c->nei_off.ensure(N + 1)) ||
         (r = c->el_count.ensure(kMaxEl + 1)) || (r = c->el_start.ensure(kMaxEl + 1)) || (r = c->el_atoms.ensure(N)) ||
         (r = c->scan_tmp.ensure(std::max<size_t>(N, ncells) / 1024 + 256)) || (r = c->status.ensure(4)) ||
         (r = c->G.ensure(N * D.nsf_max)) || (r = c->dEdG.ensure(N * D.nsf_max)) || (r = c->atE.ensure(N)) ||
@@ -647,6 +652,7 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     b.cell_cnt = c->cell_cnt.p;
     b.cell_start = c->cell_start.p;
     b.cell_atoms = c->cell_atoms.p;
+    b.posc = c->posc.p;
     b.nei_cnt = c->nei_cnt.p;
     b.nei_off = c->nei_off.p;
     b.el_count = c->el_count.p;
@@ -688,9 +694,11 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
     if ((r = mark(0))) return r;
     if (pp && pp->pad_lists && pp->e_cap > 0) {
         // capacities known: one search pass into padded rows (buffer sized by the probe)
-        if ((r = c->pad.ensure(2 * N * (size_t)pp->m_cap))) return r;
+        if ((r = c->pad.ensure(2 * N * (size_t)pp->m_cap)) || (r = c->slab.ensure(N * (size_t)kSlabStride)))
+            return r;
         b.pad = reinterpret_cast<int2*>(c->pad.p);
         b.pad_cap = pp->m_cap;
+        b.slab = c->slab.p;
     }
     if (pp && pp->dev_boxes) L += launch_molecule_boxes(b, pp->rc_list > 0.0 ? pp->rc_list : D.max_rc, st);
     L += launch_neighbour_build_a(b, D, st, pp && !pp->upload);
@@ -720,7 +728,9 @@ int run_pipeline(hdnnp_ctx* c, int nstruct, int natoms, const int32_t* Zd, const
             pp->m_cap = (((int)std::ceil(b.mmax * f) + 8) + 31) / 32 * 32;
             E = (size_t)pp->e_cap;
             b.mmax = pp->m_cap;
-            if (pp->pad_lists && (r = c->pad.ensure(2 * N * (size_t)pp->m_cap))) return r;
+            if (pp->pad_lists && ((r = c->pad.ensure(2 * N * (size_t)pp->m_cap)) ||
+                                  (r = c->slab.ensure(N * (size_t)kSlabStride))))
+                return r;
         }
     }
     if ((r = c->nei_j.ensure(E + 1)) || (r = c->nei_s.ensure(E + 1)) || (r = c->nei_rev.ensure(E + 1)) ||

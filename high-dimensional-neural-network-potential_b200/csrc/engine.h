@@ -127,6 +127,7 @@ struct Batch {
     int* cell_cnt;            // [ncells+1]
     int* cell_start;          // [ncells+1]
     int* cell_atoms;          // [natoms]
+    double4* posc;            // [natoms] wrapped position and index of cell_atoms[p] (cell order), or null
     int* nei_cnt;             // [natoms+1]
     int* nei_off;             // [natoms+1]
     int* nei_j;               // [nentries]
@@ -186,7 +187,18 @@ struct Batch {
     // arrays after the scan (pad_cap = 0: count pass, then fill pass).
     int2* pad;                // [natoms * pad_cap]
     int pad_cap;
+    // With padded rows: per atom, the row position at the start of each
+    // (jx, jy) column of its search ("slab"; K = (2 nsearch_x + 1) (2
+    // nsearch_y + 1) <= kMaxSlabs of them) and the count at the end.  The
+    // search also tags each row entry with its slab (bits 24-31 of the
+    // shift word).  The reverse entry of (i -> j) lies in the mirrored slab
+    // K - 1 - s of j's row, so the copy into the CSR arrays finds it with a
+    // scan of that slab alone.  Null: no slab table (full-row search).
+    unsigned short* slab;     // [natoms * kSlabStride]
 };
+
+constexpr int kMaxSlabs = 64;
+constexpr int kSlabStride = kMaxSlabs + 2;  // K + 1 prefix values, padded to an even count
 
 constexpr int kPairCap = 1024;  // listed pairs per atom (the dense workloads average ~550)
 

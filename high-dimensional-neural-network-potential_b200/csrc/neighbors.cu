@@ -143,6 +143,31 @@ __global__ void k_sort_cells(Batch b) {
     }
 }
 
+// Cell-ordered copy of the wrapped positions: the neighbour search reads one
+// 32-byte record per candidate instead of an index and then the position.
+__global__ void k_cell_positions(Batch b) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b.natoms || keep_list(b)) return;
+    const int j = b.cell_atoms[p];
+    b.posc[p] = make_double4(b.wpos[3 * j], b.wpos[3 * j + 1], b.wpos[3 * j + 2], __longlong_as_double((long long)j));
+}
+
+// Candidate p of the cell lists: atom index and wrapped position.
+__device__ __forceinline__ int cand(const Batch& b, int p, double& x, double& y, double& z) {
+    if (b.posc) {
+        const double4 q = b.posc[p];
+        x = q.x;
+        y = q.y;
+        z = q.z;
+        return (int)__double_as_longlong(q.w);
+    }
+    const int j = b.cell_atoms[p];
+    x = b.wpos[3 * j];
+    y = b.wpos[3 * j + 1];
+    z = b.wpos[3 * j + 2];
+    return j;
+}
+
 // floor(a / n) for n > 0, in integers (the same value as the floating-point
 // floor of the exact quotient)
 __device__ __forceinline__ int floor_div(int a, int n) { return a >= 0 ? a / n : -((n - 1 - a) / n); }
@@ -168,8 +193,13 @@ __global__ void k_neighbours(Batch b, DevModel m) {
     int n = 0;
     int out = kMode == 1 ? b.nei_off[i] : 0;
     int2* row = kMode == 2 ? b.pad + (size_t)i * b.pad_cap : nullptr;
+    // slab prefixes of the padded row (see Batch::slab)
+    const int nslab = (2 * S.nsearch[0] + 1) * (2 * S.nsearch[1] + 1);
+    unsigned short* tab = (kMode == 2 && b.slab && nslab <= kMaxSlabs) ? b.slab + (size_t)i * kSlabStride : nullptr;
+    int slab = 0;
     for (int jx = -S.nsearch[0]; jx <= S.nsearch[0]; ++jx) {
-        for (int jy = -S.nsearch[1]; jy <= S.nsearch[1]; ++jy) {
+        for (int jy = -S.nsearch[1]; jy <= S.nsearch[1]; ++jy, ++slab) {
+            if (tab) tab[slab] = (unsigned short)min(n, 0xffff);
             for (int jz = -S.nsearch[2]; jz <= S.nsearch[2]; ++jz) {
                 int cx = ix + jx, cy = iy + jy, cz = iz + jz;
                 int dx = 0, dy = 0, dz = 0;
@@ -197,9 +227,12 @@ __global__ void k_neighbours(Batch b, DevModel m) {
                 const int cell = S.cell_off + (cx * S.ngrid[1] + cy) * S.ngrid[2] + cz;
                 const int p0 = b.cell_start[cell], p1 = b.cell_start[cell + 1];
                 for (int p = p0; p < p1; ++p) {
-                    const int j = b.cell_atoms[p];
+                    double px, py, pz;
+                    const int j = cand(b, p, px, py, pz);
                     if (j == i && home) continue;
-                    double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
+                    px += lx;
+                    py += ly;
+                    pz += lz;
                     double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
                     if (ddx * ddx + ddy * ddy + ddz * ddz < rc2) {
                         if (kMode == 1) {
@@ -207,7 +240,8 @@ __global__ void k_neighbours(Batch b, DevModel m) {
                             b.nei_s[out] = pack_shift(dx, dy, dz);
                             ++out;
                         } else {
-                            if (kMode == 2 && n < b.pad_cap) row[n] = make_int2(j, pack_shift(dx, dy, dz));
+                            if (kMode == 2 && n < b.pad_cap)
+                                row[n] = make_int2(j, pack_shift(dx, dy, dz) | (tab ? slab << 24 : 0));
                             ++n;
                         }
                     }
@@ -215,6 +249,7 @@ __global__ void k_neighbours(Batch b, DevModel m) {
             }
         }
     }
+    if (tab) tab[nslab] = (unsigned short)min(n, 0xffff);
     if (kMode != 1) b.nei_cnt[i] = n;
 }
 
@@ -244,6 +279,9 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
     int n = 0;
     int out = kMode == 1 ? b.nei_off[i] : 0;
     int2* row = kMode == 2 ? b.pad + (size_t)i * b.pad_cap : nullptr;
+    // slab prefixes of the padded row (see Batch::slab): slab = v / nz
+    const int nslab = (2 * S.nsearch[0] + 1) * ny;
+    unsigned short* tab = (kMode == 2 && b.slab && nslab <= kMaxSlabs) ? b.slab + (size_t)i * kSlabStride : nullptr;
     for (int v0 = 0; v0 < nv; v0 += 32) {
         const int v = v0 + lane;
         int p0 = 0, p1 = 0, dx = 0, dy = 0, dz = 0;
@@ -283,9 +321,12 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
         // this lane's accepted atoms of its virtual cell
         int cnt = 0;
         for (int p = p0; p < p1; ++p) {
-            const int j = b.cell_atoms[p];
+            double px, py, pz;
+            const int j = cand(b, p, px, py, pz);
             if (j == i && home) continue;
-            double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
+            px += lx;
+            py += ly;
+            pz += lz;
             double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
             cnt += ddx * ddx + ddy * ddy + ddz * ddz < rc2;
         }
@@ -296,13 +337,17 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
             if (lane >= d) incl += o;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (tab && v < nv && v % nz == 0) tab[v / nz] = (unsigned short)min(n + incl - cnt, 0xffff);
         if (kMode != 0 && cnt > 0) {
             int o = (kMode == 1 ? out : n) + incl - cnt;
-            const int sh = pack_shift(dx, dy, dz);
+            const int sh = pack_shift(dx, dy, dz) | (tab ? (v / nz) << 24 : 0);
             for (int p = p0; p < p1; ++p) {
-                const int j = b.cell_atoms[p];
+                double px, py, pz;
+                const int j = cand(b, p, px, py, pz);
                 if (j == i && home) continue;
-                double px = b.wpos[3 * j] + lx, py = b.wpos[3 * j + 1] + ly, pz = b.wpos[3 * j + 2] + lz;
+                px += lx;
+                py += ly;
+                pz += lz;
                 double ddx = xi - px, ddy = yi - py, ddz = zi - pz;
                 if (ddx * ddx + ddy * ddy + ddz * ddz < rc2) {
                     if (kMode == 1) {
@@ -318,21 +363,59 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
         out += total;
         n += total;
     }
+    if (tab && lane == 0) tab[nslab] = (unsigned short)min(n, 0xffff);
     if (kMode != 1 && lane == 0) b.nei_cnt[i] = n;
 }
 
-// Padded rows -> CSR lists (plans), one warp per atom.  After an overflow the
-// capacity check has emptied the lists (nei_off all 0), so nothing is copied.
+// Padded rows -> CSR lists (plans, eager calls after the first), one warp
+// per atom, lanes over its entries; with the slab table it also writes the
+// reverse index: the entry (j -> i, -S) of (i -> j, S) found in slab s lies
+// in slab K - 1 - s of j's row (the mirrored (jx, jy) column, because j's
+// search offsets mirror i's), a scan of a few entries.  Without the table
+// (more than kMaxSlabs columns) the whole row of j is scanned.  After an
+// overflow the capacity check has emptied the lists (nei_off all 0), so
+// nothing is copied.
 __global__ void k_rows_to_lists(Batch b) {
     const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= b.natoms || keep_list(b)) return;  // uniform per warp
     const int e0 = b.nei_off[i], n = min(b.nei_off[i + 1] - e0, b.pad_cap);
     const int2* row = b.pad + (size_t)i * b.pad_cap;
+    int nslab = 0;
+    if (b.slab) {
+        const StructInfo& S = b.info[b.sid[i]];
+        nslab = (2 * S.nsearch[0] + 1) * (2 * S.nsearch[1] + 1);
+        if (nslab > kMaxSlabs) nslab = 0;
+    }
     for (int q = lane; q < n; q += 32) {
         const int2 v = row[q];
-        b.nei_j[e0 + q] = v.x;
-        b.nei_s[e0 + q] = v.y;
+        const int j = v.x, sh = v.y & 0xffffff;
+        b.nei_j[e0 + q] = j;
+        b.nei_s[e0 + q] = sh;
+        if (!b.slab) continue;
+        int sx, sy, sz;
+        unpack_shift(sh, sx, sy, sz);
+        const int want = pack_shift(-sx, -sy, -sz);
+        const int2* rj = b.pad + (size_t)j * b.pad_cap;
+        const int nj = min(b.nei_off[j + 1] - b.nei_off[j], b.pad_cap);
+        int lo = 0, hi = nj;
+        if (nslab) {
+            const int m = nslab - 1 - (int)((unsigned)v.y >> 24);
+            const unsigned short* tj = b.slab + (size_t)j * kSlabStride;
+            lo = min((int)tj[m], nj);
+            hi = min((int)tj[m + 1], nj);
+        }
+        int r = -1;
+        for (int p = lo; p < hi && r < 0; ++p) {
+            const int2 u = rj[p];
+            if (u.x == i && (u.y & 0xffffff) == want) r = p;
+        }
+        for (int p = 0; p < nj && r < 0; ++p) {  // not in its slab (should not happen): the whole row
+            const int2 u = rj[p];
+            if (u.x == i && (u.y & 0xffffff) == want) r = p;
+        }
+        if (r < 0) atomicOr(&b.status[0], 2);  // asymmetric list (should not happen)
+        b.nei_rev[e0 + q] = r < 0 ? e0 + q : b.nei_off[j] + r;
     }
 }
 
@@ -374,7 +457,7 @@ __global__ void k_reverse(Batch b, int parts) {
             if (kPad) {
                 const int2 v = b.pad[(size_t)a * b.pad_cap + (e - ea)];
                 j = v.x;
-                sh = v.y;
+                sh = v.y & 0xffffff;
             } else {
                 j = b.nei_j[e];
                 sh = b.nei_s[e];
@@ -396,7 +479,7 @@ __global__ void k_reverse(Batch b, int parts) {
             if (open && f < f1) {
                 if (kPad) {
                     const int2 v = row[fb + gl];
-                    hit = v.x == a && v.y == want;
+                    hit = v.x == a && (v.y & 0xffffff) == want;
                 } else {
                     hit = b.nei_j[f] == a && b.nei_s[f] == want;
                 }
@@ -499,6 +582,10 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, 
     ++L;
     k_sort_cells<<<(unsigned)((32LL * b.ncells + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     ++L;
+    if (b.posc) {
+        k_cell_positions<<<gA, kThreads, 0, s>>>(b);
+        ++L;
+    }
     const unsigned gW = (unsigned)((32LL * b.natoms + kThreads - 1) / kThreads);
     if (b.pad_cap > 0) {  // plans: one search pass into padded rows
         if (warp_lists(b))
@@ -522,6 +609,11 @@ int launch_neighbour_build_a(const Batch& b, const DevModel& m, cudaStream_t s, 
 int launch_neighbour_build_b(const Batch& b, const DevModel& m, cudaStream_t s) {
     const int gA = (b.natoms + kThreads - 1) / kThreads;
     const long long warps_threads = 32LL * b.natoms;
+    if (b.pad_cap > 0 && b.slab) {
+        // copy and reverse index in one pass
+        k_rows_to_lists<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
+        return 1;
+    }
     if (b.pad_cap > 0)
         k_rows_to_lists<<<(unsigned)((warps_threads + kThreads - 1) / kThreads), kThreads, 0, s>>>(b);
     else if (warp_lists(b))

@@ -250,3 +250,41 @@ def test_denser_structure_after_a_sparse_one(eng, W, abx3_model):
     assert E == E0 == E2
     assert np.array_equal(F, F0) and np.array_equal(F2, F0) and np.array_equal(dl, dl0) and np.array_equal(dl2, dl0)
     check(E, F, dl, abx3_model.eval(dense["Z"], dense["pos"], dense["lat"]))
+
+
+def test_reverse_index_of_padded_rows(eng, W):
+    """A context's second call searches into padded rows and builds the
+    reverse index while copying them (the mirrored (jx, jy) column of the
+    neighbour's row); the first call counts, fills and searches the whole
+    list.  Lists and reverse indices are the same entry for entry, for small
+    cells with multiple images, larger cells, molecules (one flat) and a cell
+    so small that its search spans more columns than the slab table holds."""
+    rng = np.random.default_rng(91)
+    structs = W.config_c4(n_struct=10, seed=19)
+    blob = W.supercell(W.abx3_cell(), (3, 1, 1))
+    structs.append({"Z": blob["Z"], "pos": blob["pos"] + rng.normal(0, 0.05, blob["pos"].shape), "lat": None})
+    flat = W.abx3_cell()
+    fp = flat["pos"].copy()
+    fp[:, 2] = 0.0
+    structs.append({"Z": flat["Z"], "pos": fp, "lat": None})
+    # a 3.6 Bohr cell: 9 x 9 search columns, more than the slab table holds
+    structs.append({"Z": np.array([1, 6], np.int32), "pos": np.array([[0.3, 0.2, 0.1], [1.9, 1.7, 2.0]]),
+                    "lat": np.eye(3) * 3.6})
+    p = eng.Hdnnp.from_runner(ABX3_DIR)
+    try:
+        p.set_option("small_eval", 0)
+        out = []
+        for _ in range(2):
+            r = p.eval_batch(structs, dEdLat=True)
+            n = sum(len(s["Z"]) for s in structs)
+            cnt = p.fetch("nei_count", n, np.int32)
+            tot = int(cnt.sum())
+            out.append((r, p.fetch("nei_index", tot, np.int32), p.fetch("nei_shift", tot, np.int32),
+                        p.fetch("nei_rev", tot, np.int32), p.launches()))
+    finally:
+        p.close()
+    (r0, j0, s0, v0, l0), (r1, j1, s1, v1, l1) = out
+    assert np.array_equal(j0, j1) and np.array_equal(s0, s1) and np.array_equal(v0, v1)
+    assert l1 < l0  # no separate reverse-index launch
+    for k in ("energy", "forces", "dEdLat"):
+        assert np.array_equal(r0[k], r1[k])
