@@ -306,13 +306,20 @@ __device__ __forceinline__ void fpair(int c, int sa, int na, int sb, int nb, boo
     }
 }
 
-// u = 1 - r_jk/rc for the pair cutoff.  Near rc the difference cancels; it
-// is formed as (rc^2 - r_jk^2) / (rc (rc + r_jk)) with rc^2 - r_jk^2 taken
-// in FP64 from the FP64 relative vectors, so that the FP32 form keeps the
-// cutoff accurate to FP32 rounding even for pairs just inside rc (whose
+// u = 1 - r_jk/rc for the pair cutoff.  In the FP32 form the difference
+// cancels near rc; it is formed as (rc^2 - r_jk^2) / (rc (rc + r_jk)) with
+// rc^2 - r_jk^2 taken in FP64 from the FP64 relative vectors, so that the
+// cutoff stays accurate to FP32 rounding even for pairs just inside rc (whose
 // SFs can have tiny scaling ranges and therefore large weights).
 template <typename T>
-__device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d, T rc, T rjk) {
+__device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d, T rc, T inv_rc, T rjk) {
+    if (sizeof(T) == 8) {
+        // FP64: 1 - r_jk / rc directly (r_jk < rc by the candidate test); its
+        // absolute error is a few ulp, which near rc only touches terms of
+        // order u^3
+        const T u = (T)1 - rjk * inv_rc;
+        return u > (T)0 ? u : (T)0;
+    }
     double cx, cy, cz;
     if (sizeof(T) == 4) {
         // FP64 relative vectors rebuilt exactly from the FP32 value and residual
@@ -418,6 +425,74 @@ __device__ __forceinline__ void powers(const DevModel& m, T X, T (&Tz)[S::NZ], T
     }
 }
 
+// Packed FP32 form of powers() for NL == 2: both lambdas of a pair in one
+// float2, X = (1 + lambda_0 cos, 1 + lambda_1 cos), squared and multiplied by
+// the paired f32x2 instructions of sm_100 (fma.rn.f32x2 / mul.rn.f32x2; each
+// half rounds exactly like the scalar instruction, so the results are those
+// of powers<S, kDeriv, float>).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+template <class S, bool kDeriv>
+__device__ __forceinline__ void powers2(const DevModel& m, float2 X, float2 (&Tz)[S::NZ], float2 (&Tp)[S::NZ]) {
+    float2 ch[5];
+    ch[0] = X;
+    if constexpr (S::kFixed) {
+        constexpr int mb = S::maxbit();
+#pragma unroll
+        for (int b = 1; b < 5; ++b) ch[b] = b <= mb ? __fmul2_rn(ch[b - 1], ch[b - 1]) : f2(0.0f);
+#pragma unroll
+        for (int z = 0; z < S::NZ; ++z) {
+            const int e = kDeriv ? S::zeta(z) - 1 : S::zeta(z);
+            float2 p = f2(1.0f);
+            bool first = true;
+#pragma unroll
+            for (int bit = 0; bit < 5; ++bit)
+                if ((e >> bit) & 1) {
+                    p = first ? ch[bit] : __fmul2_rn(p, ch[bit]);
+                    first = false;
+                }
+            if constexpr (kDeriv) {
+                Tp[z] = p;
+                Tz[z] = __fmul2_rn(p, X);
+            } else {
+                Tz[z] = p;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int b = 1; b < 5; ++b) ch[b] = b <= m.zmaxbit ? __fmul2_rn(ch[b - 1], ch[b - 1]) : f2(0.0f);
+#pragma unroll
+        for (int z = 0; z < S::NZ; ++z) {
+            float2 p = f2(0.0f), q = f2(0.0f);
+            if (z < m.fz) {
+                const int ez = m.zint[z];
+                const int e = kDeriv ? ez : ez + 1;
+                if (ez >= 0) {
+                    float2 r = f2(1.0f);
+#pragma unroll
+                    for (int bit = 0; bit < 5; ++bit)
+                        if ((e >> bit) & 1) r = __fmul2_rn(r, ch[bit]);
+                    if (kDeriv) {
+                        p = r;
+                        q = __fmul2_rn(r, X);
+                    } else {
+                        q = r;
+                    }
+                } else if (kDeriv) {
+                    const float zm = (float)m.zet[z] - 1.0f;
+                    p = make_float2(powf(X.x, zm), powf(X.y, zm));
+                    q = __fmul2_rn(p, X);
+                } else {
+                    const float zz = (float)m.zet[z];
+                    q = make_float2(powf(X.x, zz), powf(X.y, zz));
+                }
+            }
+            Tz[z] = q;
+            if (kDeriv) Tp[z] = p;
+        }
+    }
+}
+
 template <class S>
 __device__ __forceinline__ int n_eta(const DevModel& m) {
     return S::kFixed ? S::NE : m.fe;
@@ -434,6 +509,8 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
     const int nel = m.nel;
     T* Gout = Buf<T>::G(b);
     const int ne = n_eta<S>(m);
+    // work counters of this warp's atoms (profiling), added to b.stats once at the end
+    unsigned long long st_ent = 0, st_cand = 0, st_pairs = 0, st_g2 = 0;
     for (int i = blockIdx.x * kWarps + wib; i < b.natoms; i += gridDim.x * kWarps) {
         const int c = b.elem[i];
         if (c < 0) continue;
@@ -475,9 +552,15 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             const int ncand = same ? na * (na - 1) / 2 : na * nb;
             const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
             n_cand += ncand;
+            // FP32 with two lambdas: the accumulators packed over lambda,
+            // acc2[z * NE + e] = (acc[0, z, e], acc[1, z, e])
+            constexpr bool kPk = sizeof(T) == 4 && NL == 2;
             T acc[P];
+            float2 acc2[kPk ? NZ * NE : 1];
 #pragma unroll
             for (int p = 0; p < P; ++p) acc[p] = (T)0;
+#pragma unroll
+            for (int p = 0; p < (kPk ? NZ * NE : 1); ++p) acc2[p] = f2(0.0f);
             int qlen = 0;
             for (int cb = 0; cb < ncand; cb += 32) {
                 const int cidx = cb + lane;
@@ -511,7 +594,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                         const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;
                         const T rjk2 = cx * cx + cy * cy + cz * cz;
                         const T rjk = xsqrt(rjk2);
-                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk));
+                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, inv_rc, rjk));
                         const T fjk = tj * tj * tj;
                         const T t1 = -xa.z * xb.z;  // -1/(rj rk)
                         const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
@@ -520,14 +603,26 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                         T Y[NE];
 #pragma unroll
                         for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) * fcp : (T)0;
-#pragma unroll
-                        for (int l = 0; l < NL; ++l) {
-                            T Tz[NZ], Tp[NZ];
-                            powers<S, false>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+                        if constexpr (kPk) {
+                            const float2 X = __ffma2_rn(make_float2((float)m.lam[0], (float)m.lam[1]), f2((float)cth),
+                                                        f2(1.0f));
+                            float2 Tz[NZ], Tp[NZ];
+                            powers2<S, false>(m, X, Tz, Tp);
 #pragma unroll
                             for (int z = 0; z < NZ; ++z)
 #pragma unroll
-                                for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz[z] * Y[e];
+                                for (int e = 0; e < NE; ++e)
+                                    acc2[z * NE + e] = __ffma2_rn(Tz[z], f2((float)Y[e]), acc2[z * NE + e]);
+                        } else {
+#pragma unroll
+                            for (int l = 0; l < NL; ++l) {
+                                T Tz[NZ], Tp[NZ];
+                                powers<S, false>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+#pragma unroll
+                                for (int z = 0; z < NZ; ++z)
+#pragma unroll
+                                    for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz[z] * Y[e];
+                            }
                         }
                     }
                     __syncwarp();
@@ -543,8 +638,16 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             // warp reduction of acc[P] through shared memory (row stride P+1)
             {
                 T* row = s.red + lane * (P + 1);
+                if constexpr (kPk) {
 #pragma unroll
-                for (int p = 0; p < P; ++p) row[p] = acc[p];
+                    for (int q = 0; q < NZ * NE; ++q) {
+                        row[q] = (T)acc2[q].x;            // l = 0
+                        row[NZ * NE + q] = (T)acc2[q].y;  // l = 1
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < P; ++p) row[p] = acc[p];
+                }
             }
             __syncwarp();
             constexpr int NH = 32 / P > 0 ? 32 / P : 1;
@@ -565,16 +668,23 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             }
         }
         if (b.pairs && lane == 0) b.npairs[i] = n_pairs > (unsigned long long)INT32_MAX ? INT32_MAX : (int)n_pairs;
-        if (b.stats && lane == 0) {
-            unsigned long long n2 = 0;
-            for (int f = r0; f < r1; ++f) n2 += s.est[m.g2[f].nel + 1] - s.est[m.g2[f].nel];
-            atomicAdd(&b.stats[2], (unsigned long long)M);
-            atomicAdd(&b.stats[3], n_cand);
-            atomicAdd(&b.stats[4], n_pairs);
-            atomicAdd(&b.stats[5], n_pairs * (unsigned long long)P);
-            atomicAdd(&b.stats[6], n2);
+        if (b.stats) {
+            // radial terms: staged neighbours of each element x the centre's radial SFs for it
+            for (int el = 0; el < nel; ++el)
+                st_g2 += (unsigned long long)(s.est[el + 1] - s.est[el]) *
+                         (unsigned long long)(m.g2_off[c * nel + el + 1] - m.g2_off[c * nel + el]);
+            st_ent += (unsigned long long)M;
+            st_cand += n_cand;
+            st_pairs += n_pairs;
         }
         __syncwarp();
+    }
+    if (b.stats && lane == 0 && st_ent) {
+        atomicAdd(&b.stats[2], st_ent);
+        atomicAdd(&b.stats[3], st_cand);
+        atomicAdd(&b.stats[4], st_pairs);
+        atomicAdd(&b.stats[5], st_pairs * (unsigned long long)P);
+        atomicAdd(&b.stats[6], st_g2);
     }
 }
 
@@ -601,7 +711,7 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const T rjk2 = cx * cx + cy * cy + cz * cz;
             T rjk, irjk;
             dist_inv(rjk2, rjk, irjk);
-            const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, rjk)), tt = tj * tj;
+            const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, inv_rc, rjk)), tt = tj * tj;
             const T fjk = tt * tj;
             const T dfjk = (T)(-3) * inv_rc * irjk * (tt - tt * tt);
             const T irj = xa.z, irk = xb.z;
@@ -620,17 +730,41 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             T wa[P], wc[P];
             ldvec<P>(s.WA + pt * P, wa);
             ldvec<P>(s.WC + pt * P, wc);
+            if constexpr (sizeof(T) == 4 && NL == 2) {
+                // packed over lambda: the weights are staged as (l = 0, l = 1)
+                // pairs, wa[2 (z NE + e) + l] (see the staging in k_sfg_fast)
+                const float2 X = __ffma2_rn(make_float2((float)m.lam[0], (float)m.lam[1]), f2((float)cth), f2(1.0f));
+                float2 Tz[NZ], Tp[NZ];
+                powers2<S, true>(m, X, Tz, Tp);
+                float2 SA2[NE], SC2[NE];
 #pragma unroll
-            for (int l = 0; l < NL; ++l) {
-                T Tz[NZ], Tp[NZ];
-                powers<S, true>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+                for (int e = 0; e < NE; ++e) SA2[e] = SC2[e] = f2(0.0f);
 #pragma unroll
                 for (int z = 0; z < NZ; ++z)
 #pragma unroll
                     for (int e = 0; e < NE; ++e) {
-                        SA[e] += wa[(l * NZ + z) * NE + e] * Tz[z];
-                        SC[e] += wc[(l * NZ + z) * NE + e] * Tp[z];
+                        const int q = 2 * (z * NE + e);
+                        SA2[e] = __ffma2_rn(make_float2(wa[q], wa[q + 1]), Tz[z], SA2[e]);
+                        SC2[e] = __ffma2_rn(make_float2(wc[q], wc[q + 1]), Tp[z], SC2[e]);
                     }
+#pragma unroll
+                for (int e = 0; e < NE; ++e) {
+                    SA[e] = SA2[e].x + SA2[e].y;
+                    SC[e] = SC2[e].x + SC2[e].y;
+                }
+            } else {
+#pragma unroll
+                for (int l = 0; l < NL; ++l) {
+                    T Tz[NZ], Tp[NZ];
+                    powers<S, true>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+#pragma unroll
+                    for (int z = 0; z < NZ; ++z)
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) {
+                            SA[e] += wa[(l * NZ + z) * NE + e] * Tz[z];
+                            SC[e] += wc[(l * NZ + z) * NE + e] * Tp[z];
+                        }
+                }
             }
             T A = (T)0, B = (T)0, C = (T)0;
 #pragma unroll
@@ -718,13 +852,15 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fas
             const int t = q / P, p = q % P;
             const int sf = m.pmap[((size_t)c * m.nblk + t) * P + p];
             T wa = (T)0, wc = (T)0;
+            const int l = p / (NZ * NE), z = (p / NE) % NZ;
             if (sf >= 0) {
-                const int l = p / (NZ * NE), z = (p / NE) % NZ;
                 wa = (T)((double)dEdGi[sf] * iwc[sf]) * (T)m.pfz[z];
                 wc = wa * (T)m.lam[l] * (T)m.zet[z];
             }
-            s.WA[q] = wa;
-            s.WC[q] = wc;
+            // FP32 with two lambdas: (l = 0, l = 1) pairs for the packed contraction
+            const int dst = (sizeof(T) == 4 && NL == 2) ? t * P + 2 * (p % (NZ * NE)) + l : q;
+            s.WA[dst] = wa;
+            s.WC[dst] = wc;
         }
         __syncwarp();
 
