@@ -389,6 +389,17 @@ int upload_model(hdnnp_model* m) {
                     D.pfz[z] = D.zint[z] >= 0 ? std::ldexp(1.0, -D.zint[z]) : std::pow(2.0, 1.0 - zets[z]);
                 }
                 for (int e = 0; e < D.fe; ++e) D.eta4[e] = etas[e];
+                // integer eta ratios: exp(-eta_e R) = exp(-eta_0 R)^k_e
+                bool ints = D.fe > 1 && etas[0] > 0.0;
+                for (int e = 1; e < D.fe && ints; ++e) {
+                    const double k = etas[e] / etas[0], kr = std::nearbyint(k);
+                    ints = kr >= 2.0 && kr <= 64.0 && std::fabs(k - kr) <= 1e-12 * kr;
+                    D.eta_k[e] = (int)kr;
+                }
+                if (!ints)
+                    for (int e = 0; e < 8; ++e) D.eta_k[e] = 0;
+                else
+                    D.eta_k[0] = 1;
                 int bit = 0;
                 while ((1 << (bit + 1)) <= maxz) ++bit;
                 D.zmaxbit = bit;

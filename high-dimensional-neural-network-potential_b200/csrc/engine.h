@@ -92,6 +92,10 @@ struct DevModel {
     int zint[8];              // zeta - 1 if zeta is an integer >= 1, else -1
     double pfz[8];            // 2^(1 - zeta)
     double eta4[8];
+    // eta4[e] / eta4[0] when every ratio is an integer 2..64 (ascending
+    // etas), else 0: the FP64 kernels then take exp(-eta_e R) as
+    // exp(-eta_0 R)^k_e by squaring, one exponential per pair
+    int eta_k[8];
     int zmaxbit;              // highest bit of the integer zeta - 1 values
     const short* pmap;        // [nel][nblk][P]: SF index of product entry p, or -1
     // FP32 copies of the network weights (mixed-precision form)

@@ -127,11 +127,11 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // precision-dispatched math
 __device__ __forceinline__ double xsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
-// r and 1/r from r^2 > 0: FP64 by sqrt and division; FP32 by one reciprocal
-// square root (rsqrtf, 2 ulp) and a product
+// r and 1/r from r^2 > 0 by one reciprocal square root and a product: FP64
+// rsqrt (1 ulp), FP32 rsqrtf (2 ulp)
 __device__ __forceinline__ void dist_inv(double r2, double& r, double& ir) {
-    r = sqrt(r2);
-    ir = 1.0 / r;
+    ir = rsqrt(r2);
+    r = r2 * ir;
 }
 __device__ __forceinline__ void dist_inv(float r2, float& r, float& ir) {
     ir = rsqrtf(r2);
@@ -149,6 +149,35 @@ __device__ __forceinline__ double xtanh(double x) { return tanh(x); }
 __device__ __forceinline__ float xtanh(float x) { return tanhf(x); }
 __device__ __forceinline__ double xpow(double x, double y) { return pow(x, y); }
 __device__ __forceinline__ float xpow(float x, float y) { return powf(x, y); }
+
+// Y[e] = exp(-eta_e R) for the distinct etas of the grid (zero beyond ne).
+// FP64 with integer eta ratios k_e = eta_e / eta_0 (DevModel::eta_k): one
+// exponential and Y[e] = Y[0]^k_e by squaring (relative error about k_e ulp,
+// far below the FP64 tolerances); otherwise one exponential per eta.
+template <int NE, typename T>
+__device__ __forceinline__ void eta_exps(const DevModel& m, int ne, T R, T (&Y)[NE]) {
+    if (sizeof(T) == 8 && NE > 1 && m.eta_k[0] == 1) {
+        const T y0 = xexp(-(T)m.eta4[0] * R);
+        Y[0] = y0;
+#pragma unroll
+        for (int e = 1; e < NE; ++e) {
+            T r = (T)1, base = y0;
+            int k = e < ne ? m.eta_k[e] : 0;
+            if (e >= ne) r = (T)0;
+#pragma unroll
+            for (int bit = 0; bit < 7; ++bit) {
+                if (k & 1) r *= base;
+                k >>= 1;
+                if (!k) break;
+                base *= base;
+            }
+            Y[e] = r;
+        }
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) : (T)0;
+}
 
 template <typename T> struct Buf;
 template <> struct Buf<double> {
@@ -601,8 +630,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                         const T fcp = xa.x * xb.x * fjk;
                         const T R = a.w * a.w + bq.w * bq.w + rjk2;
                         T Y[NE];
+                        eta_exps<NE>(m, ne, R, Y);
 #pragma unroll
-                        for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) * fcp : (T)0;
+                        for (int e = 0; e < NE; ++e) Y[e] *= fcp;
                         if constexpr (kPk) {
                             const float2 X = __ffma2_rn(make_float2((float)m.lam[0], (float)m.lam[1]), f2((float)cth),
                                                         f2(1.0f));
@@ -723,7 +753,7 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const T R = a.w * a.w + bq.w * bq.w + rjk2;
             T Y[NE];
 #pragma unroll
-            for (int e = 0; e < NE; ++e) Y[e] = e < ne ? xexp(-(T)m.eta4[e] * R) : (T)0;
+            eta_exps<NE>(m, ne, R, Y);
             T SA[NE], SC[NE];
 #pragma unroll
             for (int e = 0; e < NE; ++e) SA[e] = SC[e] = (T)0;
