@@ -44,7 +44,7 @@ __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15);
 template <typename T>
 struct FSmem {
     V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
-    V4<float>* lo;  // FP32 form: FP64 d - (float)d per component (FP64 d = nb + lo)
+    double4* dd;    // FP32 form: the FP64 relative vector (x, y, z, -) for the pair cutoff
     V4<T>* ax;      // fc, dfc/r, 1/r, -
     V4<T>* g;       // gradient accumulators (pass 2)
     int* ent;       // entry index of a slot (pass 2)
@@ -61,7 +61,7 @@ struct FSmem {
 template <typename T>
 __host__ __device__ inline size_t fast_warp_bytes(int mm, int g2max, int nblk, int P, bool grad) {
     size_t b = a16(sizeof(V4<T>) * mm) * 2;
-    if (sizeof(T) == 4) b += a16(sizeof(V4<float>) * mm);
+    if (sizeof(T) == 4) b += a16(sizeof(double4) * mm);
     if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
     else b += a16(sizeof(T) * 32 * (P + 1));
     b += a16(mm) + 64 * sizeof(unsigned) + a16(sizeof(int) * (kMaxEl + 1)) + a16(sizeof(int) * kMaxEl);
@@ -77,7 +77,7 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int g2max, int nblk,
         return q;
     };
     s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
-    s.lo = sizeof(T) == 4 ? (V4<float>*)take(sizeof(V4<float>) * mm) : nullptr;
+    s.dd = sizeof(T) == 4 ? (double4*)take(sizeof(double4) * mm) : nullptr;
     s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
     if (grad) {
         s.g = (V4<T>*)take(sizeof(V4<T>) * mm);
@@ -298,8 +298,7 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
             }
             s.nb[slot] = V4<T>{(T)dx, (T)dy, (T)dz, (T)r};
             if (sizeof(T) == 4)
-                s.lo[slot] = V4<float>{(float)(dx - (double)(float)dx), (float)(dy - (double)(float)dy),
-                                       (float)(dz - (double)(float)dz), 0.0f};
+                s.dd[slot] = make_double4(dx, dy, dz, 0.0);
             s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)ir, (T)0};
             s.el[slot] = (unsigned char)el;
             if (kGrad) {
@@ -351,12 +350,11 @@ __device__ __forceinline__ T pair_u(const FSmem<T>& s, int j, int k, double rc2d
     }
     double cx, cy, cz;
     if (sizeof(T) == 4) {
-        // FP64 relative vectors rebuilt exactly from the FP32 value and residual
-        const V4<T> a = s.nb[j], b = s.nb[k];
-        const V4<float> al = s.lo[j], bl = s.lo[k];
-        cx = ((double)b.x + (double)bl.x) - ((double)a.x + (double)al.x);
-        cy = ((double)b.y + (double)bl.y) - ((double)a.y + (double)al.y);
-        cz = ((double)b.z + (double)bl.z) - ((double)a.z + (double)al.z);
+        // the FP64 relative vectors staged beside the FP32 ones
+        const double4 a = s.dd[j], b = s.dd[k];
+        cx = b.x - a.x;
+        cy = b.y - a.y;
+        cz = b.z - a.z;
     } else {
         const V4<T> a = s.nb[j], b = s.nb[k];
         cx = (double)b.x - (double)a.x;
