@@ -569,101 +569,69 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         }
 
         unsigned long long n_cand = 0, n_pairs = 0;
-        for (int t = 0; t < m.nblk; ++t) {
-            const int gb = m.g4_off[c * m.nblk + t], ge = m.g4_off[c * m.nblk + t + 1];
-            if (ge == gb) continue;
-            const int ea = m.blk_a[t], eb = m.blk_b[t];
-            const int sa = s.est[ea], na = s.est[ea + 1] - sa;
-            const int sb = s.est[eb], nb = s.est[eb + 1] - sb;
-            const bool same = (ea == eb);
-            const int ncand = same ? na * (na - 1) / 2 : na * nb;
-            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
-            n_cand += ncand;
-            // FP32 with two lambdas: the accumulators packed over lambda,
-            // acc2[z * NE + e] = (acc[0, z, e], acc[1, z, e])
-            constexpr bool kPk = sizeof(T) == 4 && NL == 2;
-            T acc[P];
-            float2 acc2[kPk ? NZ * NE : 1];
+        // Contributing pairs of all element-pair blocks go through one queue
+        // (entries j | k << 10 | block << 20, enumeration order), so a chunk of
+        // 32 pairs may hold the end of one block and the start of the next:
+        // the lanes of the older block add their terms, every lane writes its
+        // sums of that block for the reduction (the newer block's lanes the
+        // sums they held before this chunk), and then the newer block's lanes
+        // start their sums with their terms.  The queue holds at most two
+        // blocks, and a block's remainder is carried into the next block's
+        // chunks instead of being flushed as a partly filled chunk.
+        // FP32 with two lambdas: the accumulators packed over lambda,
+        // acc2[z * NE + e] = (acc[0, z, e], acc[1, z, e]).
+        constexpr bool kPk = sizeof(T) == 4 && NL == 2;
+        T acc[P];
+        float2 acc2[kPk ? NZ * NE : 1];
+        auto zero_acc = [&]() {
 #pragma unroll
             for (int p = 0; p < P; ++p) acc[p] = (T)0;
 #pragma unroll
             for (int p = 0; p < (kPk ? NZ * NE : 1); ++p) acc2[p] = f2(0.0f);
-            int qlen = 0;
-            for (int cb = 0; cb < ncand; cb += 32) {
-                const int cidx = cb + lane;
-                bool ok = cidx < ncand;
-                int j = 0, k = 0;
-                if (ok) {
-                    fpair(cidx, sa, na, sb, nb, same, inv_nb, j, k);
-                    const V4<T> a = s.nb[j], bb = s.nb[k];
-                    const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
-                    ok = ex * ex + ey * ey + ez * ez < rc2;
-                }
-                const unsigned bal = __ballot_sync(kFull, ok);
-                if (ok) s.queue[qlen + __popc(bal & lanemask_lt())] = (unsigned)j | ((unsigned)k << 16);
-                if (ok && b.pairs) {
-                    // contributing-pair list for the gradient pass (enumeration order)
-                    const long long slot = (long long)n_pairs + __popc(bal & lanemask_lt());
-                    if (slot < b.pcap)
-                        b.pairs[(size_t)i * b.pcap + slot] = (unsigned)j | ((unsigned)k << 10) | ((unsigned)t << 20);
-                }
-                qlen += __popc(bal);
-                n_pairs += __popc(bal);
-                __syncwarp();
-                const bool last = cb + 32 >= ncand;
-                while (qlen >= 32 || (last && qlen > 0)) {
-                    const int n = qlen < 32 ? qlen : 32;
-                    if (lane < n) {
-                        const unsigned pk = s.queue[lane];
-                        const int pj = pk & 0xffff, pq = pk >> 16;
-                        const V4<T> a = s.nb[pj], bq = s.nb[pq];
-                        const V4<T> xa = s.ax[pj], xb = s.ax[pq];
-                        const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;
-                        const T rjk2 = cx * cx + cy * cy + cz * cz;
-                        const T rjk = xsqrt(rjk2);
-                        const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, inv_rc, rjk));
-                        const T fjk = tj * tj * tj;
-                        const T t1 = -xa.z * xb.z;  // -1/(rj rk)
-                        const T cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
-                        const T fcp = xa.x * xb.x * fjk;
-                        const T R = a.w * a.w + bq.w * bq.w + rjk2;
-                        T Y[NE];
-                        eta_exps<NE>(m, ne, R, Y);
+        };
+        // terms of one pair: cos(theta) and Y[e] = exp(-eta_e R) fc_ij fc_ik fc_jk
+        auto pair_terms = [&](unsigned pk, T& cth, T (&Y)[NE]) {
+            const int pj = pk & 0x3ff, pq = (pk >> 10) & 0x3ff;
+            const V4<T> a = s.nb[pj], bq = s.nb[pq];
+            const V4<T> xa = s.ax[pj], xb = s.ax[pq];
+            const T cx = bq.x - a.x, cy = bq.y - a.y, cz = bq.z - a.z;
+            const T rjk2 = cx * cx + cy * cy + cz * cz;
+            const T rjk = xsqrt(rjk2);
+            const T tj = xtanh(pair_u(s, pj, pq, rc2d, rc, inv_rc, rjk));
+            const T fjk = tj * tj * tj;
+            const T t1 = -xa.z * xb.z;  // -1/(rj rk)
+            cth = (T)0.5 * (rjk2 - a.w * a.w - bq.w * bq.w) * t1;
+            const T fcp = xa.x * xb.x * fjk;
+            const T R = a.w * a.w + bq.w * bq.w + rjk2;
+            eta_exps<NE>(m, ne, R, Y);
 #pragma unroll
-                        for (int e = 0; e < NE; ++e) Y[e] *= fcp;
-                        if constexpr (kPk) {
-                            const float2 X = __ffma2_rn(make_float2((float)m.lam[0], (float)m.lam[1]), f2((float)cth),
-                                                        f2(1.0f));
-                            float2 Tz[NZ], Tp[NZ];
-                            powers2<S, false>(m, X, Tz, Tp);
+            for (int e = 0; e < NE; ++e) Y[e] *= fcp;
+        };
+        // acc[l, z, e] += (1 + lambda_l cos)^zeta_z Y[e]
+        auto accumulate = [&](T cth, const T (&Y)[NE]) {
+            if constexpr (kPk) {
+                const float2 X = __ffma2_rn(make_float2((float)m.lam[0], (float)m.lam[1]), f2((float)cth), f2(1.0f));
+                float2 Tz[NZ], Tp[NZ];
+                powers2<S, false>(m, X, Tz, Tp);
 #pragma unroll
-                            for (int z = 0; z < NZ; ++z)
+                for (int z = 0; z < NZ; ++z)
 #pragma unroll
-                                for (int e = 0; e < NE; ++e)
-                                    acc2[z * NE + e] = __ffma2_rn(Tz[z], f2((float)Y[e]), acc2[z * NE + e]);
-                        } else {
+                    for (int e = 0; e < NE; ++e) acc2[z * NE + e] = __ffma2_rn(Tz[z], f2((float)Y[e]), acc2[z * NE + e]);
+            } else {
 #pragma unroll
-                            for (int l = 0; l < NL; ++l) {
-                                T Tz[NZ], Tp[NZ];
-                                powers<S, false>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
+                for (int l = 0; l < NL; ++l) {
+                    T Tz[NZ], Tp[NZ];
+                    powers<S, false>(m, (T)1 + (T)m.lam[l] * cth, Tz, Tp);
 #pragma unroll
-                                for (int z = 0; z < NZ; ++z)
+                    for (int z = 0; z < NZ; ++z)
 #pragma unroll
-                                    for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz[z] * Y[e];
-                            }
-                        }
-                    }
-                    __syncwarp();
-                    const int rem = qlen - n;
-                    unsigned v = 0;
-                    if (lane < rem) v = s.queue[n + lane];
-                    __syncwarp();
-                    if (lane < rem) s.queue[lane] = v;
-                    __syncwarp();
-                    qlen = rem;
+                        for (int e = 0; e < NE; ++e) acc[(l * NZ + z) * NE + e] += Tz[z] * Y[e];
                 }
             }
-            // warp reduction of acc[P] through shared memory (row stride P+1)
+        };
+        // every lane's sums of block t -> G of block t (warp reduction through
+        // shared memory, row stride P+1); called by all lanes
+        auto emit = [&](int t) {
             {
                 T* row = s.red + lane * (P + 1);
                 if constexpr (kPk) {
@@ -694,6 +662,96 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                     Gi[sf] = (T)(((double)((T)m.pfz[z] * sum) - mean[sf]) * iwidth[sf]);
                 }
             }
+        };
+        int qlen = 0;   // pending queue entries
+        int cur = -1;   // block whose sums the accumulators hold
+        zero_acc();
+        // process the first n queue entries (all lanes call)
+        auto flush = [&](int n) {
+            const unsigned pk = lane < n ? s.queue[lane] : 0u;
+            const int tg = lane < n ? (int)(pk >> 20) : cur;
+            T cth = (T)0, Y[NE];
+#pragma unroll
+            for (int e = 0; e < NE; ++e) Y[e] = (T)0;
+            if (lane < n) pair_terms(pk, cth, Y);
+            if (!__any_sync(kFull, tg != cur)) {
+                if (lane < n) accumulate(cth, Y);
+            } else {
+                // the chunk ends block cur and starts the next one (the last lane's)
+                const int nxt = __shfl_sync(kFull, tg, n - 1);
+                if (lane < n && tg == cur) accumulate(cth, Y);
+                emit(cur);
+                zero_acc();
+                if (lane < n && tg == nxt) accumulate(cth, Y);
+                cur = nxt;
+            }
+            __syncwarp();
+            const int rem = qlen - n;
+            unsigned v = 0;
+            if (lane < rem) v = s.queue[n + lane];
+            __syncwarp();
+            if (lane < rem) s.queue[lane] = v;
+            __syncwarp();
+            qlen = rem;
+        };
+        for (int t = 0; t < m.nblk; ++t) {
+            const int gb = m.g4_off[c * m.nblk + t], ge = m.g4_off[c * m.nblk + t + 1];
+            if (ge == gb) continue;
+            if (cur < 0) cur = t;
+            const int ea = m.blk_a[t], eb = m.blk_b[t];
+            const int sa = s.est[ea], na = s.est[ea + 1] - sa;
+            const int sb = s.est[eb], nb = s.est[eb + 1] - sb;
+            const bool same = (ea == eb);
+            const int ncand = same ? na * (na - 1) / 2 : na * nb;
+            const float inv_nb = nb > 0 ? 1.0f / (float)nb : 0.0f;
+            n_cand += ncand;
+            for (int cb = 0; cb < ncand; cb += 32) {
+                const int cidx = cb + lane;
+                bool ok = cidx < ncand;
+                int j = 0, k = 0;
+                if (ok) {
+                    fpair(cidx, sa, na, sb, nb, same, inv_nb, j, k);
+                    const V4<T> a = s.nb[j], bb = s.nb[k];
+                    const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
+                    ok = ex * ex + ey * ey + ez * ez < rc2;
+                }
+                const unsigned bal = __ballot_sync(kFull, ok);
+                const unsigned ent = (unsigned)j | ((unsigned)k << 10) | ((unsigned)t << 20);
+                if (ok) s.queue[qlen + __popc(bal & lanemask_lt())] = ent;
+                if (ok && b.pairs) {
+                    // contributing-pair list for the gradient pass (enumeration order)
+                    const long long slot = (long long)n_pairs + __popc(bal & lanemask_lt());
+                    if (slot < b.pcap) b.pairs[(size_t)i * b.pcap + slot] = ent;
+                }
+                qlen += __popc(bal);
+                n_pairs += __popc(bal);
+                __syncwarp();
+                while (qlen >= 32) flush(32);
+            }
+            // block t is screened.  An older block still pending in the queue
+            // (its remainder followed by t's pairs, fewer than 32 together) is
+            // finished now, and then t with it.
+            if (cur != t) {
+                if (qlen > 0) flush(qlen);
+                if (cur != t) {  // t had no contributing pairs
+                    emit(cur);
+                    zero_acc();
+                    cur = t;
+                }
+                if (qlen > 0) flush(qlen);
+                emit(t);
+                zero_acc();
+                cur = -1;
+            } else if (qlen == 0) {
+                emit(t);
+                zero_acc();
+                cur = -1;
+            }
+        }
+        if (cur >= 0) {
+            if (qlen > 0) flush(qlen);
+            emit(cur);
+            zero_acc();
         }
         if (b.pairs && lane == 0) b.npairs[i] = n_pairs > (unsigned long long)INT32_MAX ? INT32_MAX : (int)n_pairs;
         if (b.stats) {
