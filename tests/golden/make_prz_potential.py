@@ -5,7 +5,8 @@ the reference the ABX3 and example potentials leave out (tests/golden/prz/):
   (activate / deactivate, neuralNetworks.f90:45-49 and :69-80);
 * angular symmetry functions with non-integer zeta (the real-power branch of
   calcAllSymmetryFunctions, symmetryFunctions.f90:266-273): zeta in
-  {1, 2.5, 6.3} x lambda +-1 x eta {0.001, 0.01} for each of the 15 element
+  {1, 2.5, 6.3} x lambda +-1 x eta {0.001, 0.013} (a non-integer eta ratio:
+  the FP64 kernels take one exponential per eta) for each of the 15 element
   pairs of H, C, N, I, Pb, plus 3 radial functions per neighbour element
   (eta 0.002, 0.05, 0.4; Rs 0): 15 + 180 = 195 per element, rc 11 Bohr,
   tanh^3 cutoff (cutoff_type 2).
@@ -43,7 +44,7 @@ def rows():
             for eta in (0.002, 0.05, 0.4):
                 out.append((c, 2, e, 0, eta, 0.0, 0.0))
         for a, b in itertools.combinations_with_replacement(els, 2):
-            for eta in (0.001, 0.01):
+            for eta in (0.001, 0.013):
                 for lam in (-1.0, 1.0):
                     for zeta in (1.0, 2.5, 6.3):
                         out.append((c, 3, a, b, eta, lam, zeta))
