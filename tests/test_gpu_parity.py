@@ -73,6 +73,7 @@ def test_flat_and_linear_molecules(eng, gex, ex_model, c1, pkg):
     # the oracle searches every cell like the reference, which for the
     # linear molecule means ~10^10 empty cells: it gets a rotated copy
     R, _ = np.linalg.qr(np.random.default_rng(5).normal(size=(3, 3)))
+    gex.set_option("small_eval", 0)  # the general pipeline, compared bitwise with the plan below
     for Z, pos, rot in ((s["Z"], flat, np.eye(3)), (s["Z"][:2], two, R)):
         E, F, _ = gex.energy_and_forces(eng.AtStruct(Z, pos))
         ref = ex_model.eval(Z, pos @ rot.T)
@@ -80,6 +81,7 @@ def test_flat_and_linear_molecules(eng, gex, ex_model, c1, pkg):
         with PL.Plan(gex, [{"Z": Z, "pos": pos, "lat": None}]) as p:  # device-built box
             Ep, Fp, _ = p.results()
         assert Ep[0] == E and np.array_equal(Fp, F)
+    gex.set_option("small_eval", 1)
 
 
 def test_crowded_cell_of_a_sparse_molecule(eng, gab, abx3_model):

@@ -87,6 +87,7 @@ def test_md_matches_host_verlet_molecule(pkg, S, W, c1):
 
     s, m, p0 = c1
     p = engine.Hdnnp.from_runner(EXAMPLE_DIR)
+    p.set_option("small_eval", 0)  # the plain calls through the pipeline the server runs (bitwise below)
     dt, nsteps = 20.0, 10
     ats = engine.AtStruct(s["Z"], s["pos"].copy())
     E0, F, _ = p.energy_and_forces(ats)
