@@ -172,6 +172,23 @@ __device__ __forceinline__ int cand(const Batch& b, int p, double& x, double& y,
 // floor of the exact quotient)
 __device__ __forceinline__ int floor_div(int a, int n) { return a >= 0 ? a / n : -((n - 1 - a) / n); }
 
+// Wrap a cell coordinate c into [0, n) and return the image count floor(c / n):
+// the search offsets reach at most nsearch cells beyond the grid, so this is
+// one step for grids of at least nsearch cells and a few for tiny cells --
+// the same result as floor_div without an integer division.
+__device__ __forceinline__ int wrap_cell(int& c, int n) {
+    int d = 0;
+    while (c < 0) {
+        c += n;
+        --d;
+    }
+    while (c >= n) {
+        c -= n;
+        ++d;
+    }
+    return d;
+}
+
 // K3 enumeration shared by the passes.  kMode 0: count; 1: fill the CSR
 // lists at nei_off; 2 (plans): count and fill the atom's padded row of
 // pad_cap entries in one pass (entries beyond pad_cap are counted only; the
@@ -198,25 +215,22 @@ __global__ void k_neighbours(Batch b, DevModel m) {
     unsigned short* tab = (kMode == 2 && b.slab && nslab <= kMaxSlabs) ? b.slab + (size_t)i * kSlabStride : nullptr;
     int slab = 0;
     for (int jx = -S.nsearch[0]; jx <= S.nsearch[0]; ++jx) {
+        // x and y of the virtual cell are wrapped once per column, z per cell
+        int cx = ix + jx;
+        const bool xin = cx >= 0 && cx < S.ngrid[0];
+        const int dx = xin ? 0 : wrap_cell(cx, S.ngrid[0]);
         for (int jy = -S.nsearch[1]; jy <= S.nsearch[1]; ++jy, ++slab) {
             if (tab) tab[slab] = (unsigned short)min(n, 0xffff);
+            int cy = iy + jy;
+            const bool yin = cy >= 0 && cy < S.ngrid[1];
+            const int dy = yin ? 0 : wrap_cell(cy, S.ngrid[1]);
+            if (!S.periodic && !(xin && yin)) continue;  // a molecule: no cells beyond its grid
             for (int jz = -S.nsearch[2]; jz <= S.nsearch[2]; ++jz) {
-                int cx = ix + jx, cy = iy + jy, cz = iz + jz;
-                int dx = 0, dy = 0, dz = 0;
+                int cz = iz + jz;
+                int dz = 0;
                 if (cz < 0 || cz >= S.ngrid[2]) {
                     if (!S.periodic) continue;
-                    dz = floor_div(cz, S.ngrid[2]);
-                    cz -= S.ngrid[2] * dz;
-                }
-                if (cy < 0 || cy >= S.ngrid[1]) {
-                    if (!S.periodic) continue;
-                    dy = floor_div(cy, S.ngrid[1]);
-                    cy -= S.ngrid[1] * dy;
-                }
-                if (cx < 0 || cx >= S.ngrid[0]) {
-                    if (!S.periodic) continue;
-                    dx = floor_div(cx, S.ngrid[0]);
-                    cx -= S.ngrid[0] * dx;
+                    dz = wrap_cell(cz, S.ngrid[2]);
                 }
                 // image shift, summed z, y, x like the reference
                 double lx = 0, ly = 0, lz = 0;
@@ -295,18 +309,15 @@ __global__ void k_neighbours_warp(Batch b, DevModel m) {
             bool inside = true;
             if (cz < 0 || cz >= S.ngrid[2]) {
                 inside = S.periodic;
-                dz = floor_div(cz, S.ngrid[2]);
-                cz -= S.ngrid[2] * dz;
+                dz = wrap_cell(cz, S.ngrid[2]);
             }
             if (cy < 0 || cy >= S.ngrid[1]) {
                 inside = inside && S.periodic;
-                dy = floor_div(cy, S.ngrid[1]);
-                cy -= S.ngrid[1] * dy;
+                dy = wrap_cell(cy, S.ngrid[1]);
             }
             if (cx < 0 || cx >= S.ngrid[0]) {
                 inside = inside && S.periodic;
-                dx = floor_div(cx, S.ngrid[0]);
-                cx -= S.ngrid[0] * dx;
+                dx = wrap_cell(cx, S.ngrid[0]);
             }
             if (inside) {
                 if (dz) { lx += h[6] * dz; ly += h[7] * dz; lz += h[8] * dz; }
