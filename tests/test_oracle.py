@@ -200,3 +200,30 @@ def test_golden_fixtures(ex_model, abx3_model, c1, W):
     assert abs(r["energy"] - fx["cell"]["energy"]) < 1e-12 * abs(fx["cell"]["energy"])
     assert np.abs(r["forces"] - np.array(fx["cell"]["forces"])).max() < 1e-11
     assert np.abs(r["dEdLat"] - np.array(fx["cell"]["dEdLat"])).max() < 1e-11
+
+
+def test_reference_double_wrap_of_face_atoms(abx3_model, W):
+    """A quirk of the reference the oracle keeps: hdnnpCalcNeighborLists wraps
+    a periodic structure (hdnnps.f90:379-386) and buildNeighborListGrid wraps
+    that copy again (neighborLists.f90:157), but takes each centre's own
+    position from the first copy (:125) and its neighbours from the second.
+    For an atom whose fractional coordinate rounds to 1.0 in the first wrap
+    the second wrap moves it by a lattice vector, so its environment is seen
+    with inconsistent images.  The unjittered strained ABX3 lattice has such
+    atoms (fractional 0 to rounding): there the grid path's energy per atom
+    depends on the supercell size, while a rigidly translated copy (no atom on
+    a face) and the brute-force list (neighborLists.f90:21-81, one wrap) agree
+    with each other for every size.  The engine wraps once, as the translated
+    copy."""
+    shift = np.array([0.0137, 0.0213, 0.0071])
+    per_atom = []
+    for n in (2, 3):
+        s = W.config_c3(n=n)
+        nat = len(s["Z"])
+        grid = abx3_model.eval(s["Z"], s["pos"], s["lat"])["energy"] / nat
+        moved = abx3_model.eval(s["Z"], s["pos"] + shift, s["lat"])["energy"] / nat
+        brute = abx3_model.eval(s["Z"], s["pos"], s["lat"], brute=True)["energy"] / nat
+        assert abs(moved - brute) <= 1e-12 * abs(brute)
+        per_atom.append((grid, moved))
+    assert abs(per_atom[0][1] - per_atom[1][1]) <= 1e-12 * abs(per_atom[0][1])  # translated: size-independent
+    assert abs(per_atom[0][0] - per_atom[0][1]) > 1e-4 * abs(per_atom[0][1])  # the quirk shows on the lattice
