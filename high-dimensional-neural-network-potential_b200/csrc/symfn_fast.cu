@@ -555,17 +555,61 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         const double* mean = m.smean + (size_t)c * m.nsf_max;
         const double* iwidth = m.sinvw + (size_t)c * m.nsf_max;
 
-        // radial SFs: lane = SF
         const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
-        for (int f = r0 + lane; f < r1; f += 32) {
-            const SF2 q = m.g2[f];
-            const T eta = (T)q.eta, rs = (T)q.rs;
-            T acc = (T)0;
-            for (int t = s.est[q.nel]; t < s.est[q.nel + 1]; ++t) {
-                const T x = s.nb[t].w - rs;
-                acc += xexp(-eta * x * x) * s.ax[t].x;
+        const int Q = m.g2q;
+        if (Q > 0 && r1 - r0 <= 32 * (P + 1)) {
+            // radial SFs: a lane per (neighbour, SF of its element), 32 / Q
+            // neighbours per round; the sums go to the centre's radial slots
+            // in s.red (free until the angular part).  A round inside one
+            // element is summed over its neighbours by shuffles, a round across
+            // an element boundary neighbour by neighbour.
+            const int R = 32 / Q, sub = lane / Q, qi = lane % Q;
+            T* racc = s.red;
+            for (int f = lane; f < r1 - r0; f += 32) racc[f] = (T)0;
+            __syncwarp();
+            for (int base = 0; base < Ms; base += R) {
+                const int t = base + sub;
+                T term = (T)0;
+                int slot = -1;
+                if (t < Ms) {
+                    const int el = s.el[t];
+                    const int f0 = m.g2_off[c * nel + el], n2 = m.g2_off[c * nel + el + 1] - f0;
+                    if (qi < n2) {
+                        const SF2 q = m.g2[f0 + qi];
+                        const T x = s.nb[t].w - (T)q.rs;
+                        term = xexp(-(T)q.eta * x * x) * s.ax[t].x;
+                        slot = f0 + qi - r0;
+                    }
+                }
+                const bool one = base + R <= Ms && s.el[base] == s.el[base + R - 1];  // uniform
+                if (one) {
+                    for (int o = Q; o < 32; o <<= 1) term += __shfl_xor_sync(kFull, term, o);
+                    if (sub == 0 && slot >= 0) racc[slot] += term;
+                } else {
+                    for (int u = 0; u < R; ++u) {
+                        if (sub == u && slot >= 0) racc[slot] += term;
+                        __syncwarp();
+                    }
+                }
+                __syncwarp();
             }
-            Gi[q.sf] = (T)(((double)acc - mean[q.sf]) * iwidth[q.sf]);
+            for (int f = r0 + lane; f < r1; f += 32) {
+                const int sf = m.g2[f].sf;
+                Gi[sf] = (T)(((double)racc[f - r0] - mean[sf]) * iwidth[sf]);
+            }
+            __syncwarp();
+        } else {
+            // radial SFs: lane = SF
+            for (int f = r0 + lane; f < r1; f += 32) {
+                const SF2 q = m.g2[f];
+                const T eta = (T)q.eta, rs = (T)q.rs;
+                T acc = (T)0;
+                for (int t = s.est[q.nel]; t < s.est[q.nel + 1]; ++t) {
+                    const T x = s.nb[t].w - rs;
+                    acc += xexp(-eta * x * x) * s.ax[t].x;
+                }
+                Gi[q.sf] = (T)(((double)acc - mean[q.sf]) * iwidth[q.sf]);
+            }
         }
 
         unsigned long long n_cand = 0, n_pairs = 0;
