@@ -244,6 +244,9 @@ def roofline(stage_ms, counters, peaks, precision, hbm_gbs):
     peak_key = "fp64" if precision == "fp64" else "fp32"
     peak = peaks.get(peak_key)
     sf_ms = ms["sf_values"] + ms["sf_gradients"]
+    if not sf_ms > 0:
+        return {"bound": peak_key + "-alu", "kernel": "sf_values + sf_gradients", "achieved": None, "peak": peak,
+                "unit": "TFLOP/s", "frac": None, "note": "no stage times recorded"}
     alg = sum(FLOPS_ALGORITHMIC[k] * per_step[k] for k in FLOPS_ALGORITHMIC)
     achieved = alg / (sf_ms / 1e3) / 1e12
     step_ms = sum(ms.values())
@@ -751,7 +754,7 @@ def main():
             oplan.launch(stream.cuda_stream)
         oplan.sync(stream.cuda_stream)
         oplan.profile(reset=True)
-        ot = timed_device_steps(max(nk, args.steps // 2), plan=oplan)
+        ot = timed_device_steps(max(nk, args.steps // 2), fn=lambda: oplan.launch(stream.cuda_stream), plan=oplan)
         oplan.sync(stream.cuda_stream)
         osec = sum(a.elapsed_time(b) for a, b in ot) / 1e3
         ost, ocnt = oplan.profile(reset=True)

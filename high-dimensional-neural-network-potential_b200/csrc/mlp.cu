@@ -1,4 +1,5 @@
-// mlp.cu -- K5: per-element atomic networks, forward pass and dE/dG (FP64).
+// mlp.cu -- K5: per-element atomic networks, forward pass and dE/dG (FP64
+// on the FP64 tensor cores, FP32 on the CUDA cores).
 //
 // Same arithmetic as nn_forward / nn_backward(gradOut = 1) per atom
 // (neuralNetworks.f90:94-158, 220-313; called from hdnnps.f90:523-531):
@@ -71,6 +72,176 @@ __global__ void __launch_bounds__(kThreads) k_mlp(Batch b, DevModel m, int maxw)
     mlp_tile<T>(b, m, maxw, e, t0, cnt, sm_raw);
 }
 
+// ---------------------------------------------------------------- FP64 tensor cores
+// The FP64 networks on the FP64 tensor cores: mma.sync m8n8k4 f64 (tcgen05
+// has no FP64 kind), a warp per 8 atoms of one element.  The first layer's
+// GEMM (8 x nin) x (nin x 32) and the input gradient dE/dG = delta_1 W_1,
+// (8 x 32) x (32 x nin), carry ~90 % of the multiply-adds; the hidden and
+// output layers (widths <= 32) run on the lanes from shared memory.  Same
+// formulas as mlp_tile (neuralNetworks.f90:94-158); the sums of the two
+// GEMMs run in the tensor cores' order.
+//   fragments (thread t): A[t/4][t%4], B[k = t%4][n = t/4],
+//   C[t/4][2 (t%4) + v], v = 0, 1
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double bb) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(bb));
+}
+
+constexpr int kDW = 4;   // warps per block
+constexpr int kDH = 32;  // widest layer the kernel takes
+constexpr int kDR = 8;   // atoms per warp
+constexpr int kDS = kDH + 1;  // row stride of the per-warp activation rows
+
+// per warp: c_l and y_l of every layer and two delta buffers, [8][kDS] each
+__host__ __device__ inline int dmma_warp_doubles(int L) { return (2 * L + 2) * kDR * kDS; }
+
+__global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
+    extern __shared__ __align__(16) double dsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int L = m.nlayers;
+    // locate (element, tile of 8 atoms) of this warp
+    int tile = blockIdx.x * kDW + wib, e = -1, t0 = 0, cnt = 0;
+    for (int x = 0; x < m.nel; ++x) {
+        const int n = b.el_start[x + 1] - b.el_start[x];
+        const int nt = (n + kDR - 1) / kDR;
+        if (tile < nt) {
+            e = x;
+            t0 = b.el_start[x] + tile * kDR;
+            cnt = min(kDR, n - tile * kDR);
+            break;
+        }
+        tile -= nt;
+    }
+    if (e < 0) return;  // uniform per warp
+    double* ws = dsm + (size_t)wib * dmma_warp_doubles(L);
+    // c_l and y_l of layer l (0-based)
+    auto cb = [&](int l) { return ws + (2 * l) * kDR * kDS; };
+    auto yb = [&](int l) { return ws + (2 * l + 1) * kDR * kDS; };
+    double* dcur = ws + (2 * L) * kDR * kDS;
+    double* dnext = dcur + kDR * kDS;
+    const int r = lane >> 2, q = lane & 3;
+    const int atom = r < cnt ? b.el_atoms[t0 + r] : -1;
+    const int nin = m.nin_el[e], nsf = m.nsf_max, H1 = m.width[1];
+    const double* W1 = m.w + m.w_off[e * L];  // [H1][nin]
+
+    // layer 1: C[8 x 32] = G[8 x nin] W1^T on the tensor cores
+    double acc[4][2];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
+    const double* grow = atom >= 0 ? b.G + (size_t)atom * nsf : nullptr;
+    for (int k0 = 0; k0 < nin; k0 += 4) {
+        const int k = k0 + q;
+        const double a = (grow && k < nin) ? grow[k] : 0.0;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int n = nt * 8 + r;  // B[k][n] = W1[n][k]
+            const double bb = (n < H1 && k < nin) ? W1[(size_t)n * nin + k] : 0.0;
+            dmma(acc[nt], a, bb);
+        }
+    }
+    {
+        const double* b1 = m.b + m.b_off[e * L];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                const int col = nt * 8 + 2 * q + v;
+                double cv = 0.0, yv = 0.0;
+                if (col < H1) {
+                    cv = acc[nt][v] + b1[col];
+                    yv = act_f(m.act[0], cv);
+                }
+                cb(0)[r * kDS + col] = cv;
+                yb(0)[r * kDS + col] = yv;
+            }
+    }
+    __syncwarp();
+    // hidden and output layers: lane = output neuron, the warp's 8 atoms
+    for (int l = 1; l < L; ++l) {
+        const int win = m.width[l], wout = m.width[l + 1];
+        const double* W = m.w + m.w_off[e * L + l];  // [wout][win]
+        const double* bl = m.b + m.b_off[e * L + l];
+        if (lane < wout) {
+            double sacc[kDR];
+#pragma unroll
+            for (int rr = 0; rr < kDR; ++rr) sacc[rr] = 0.0;
+            for (int i = 0; i < win; ++i) {
+                const double w = W[(size_t)lane * win + i];
+#pragma unroll
+                for (int rr = 0; rr < kDR; ++rr) sacc[rr] += w * yb(l - 1)[rr * kDS + i];
+            }
+#pragma unroll
+            for (int rr = 0; rr < kDR; ++rr) {
+                const double cv = sacc[rr] + bl[lane];
+                cb(l)[rr * kDS + lane] = cv;
+                yb(l)[rr * kDS + lane] = act_f(m.act[l], cv);
+            }
+        }
+        __syncwarp();
+    }
+    // atomic energies
+    if (lane < cnt) b.atE[b.el_atoms[t0 + lane]] = yb(L - 1)[lane * kDS] + m.atom_energy[e];
+    // backward: delta of the output layer (gradOut = 1), then down to layer 1
+    {
+        const int w = m.width[L];
+        if (lane < w)
+#pragma unroll
+            for (int rr = 0; rr < kDR; ++rr)
+                dcur[rr * kDS + lane] = act_d(m.act[L - 1], cb(L - 1)[rr * kDS + lane], yb(L - 1)[rr * kDS + lane]);
+    }
+    __syncwarp();
+    for (int l = L - 1; l >= 1; --l) {
+        const int wout = m.width[l + 1], wi = m.width[l];
+        const double* W = m.w + m.w_off[e * L + l];  // [wout][wi]
+#pragma unroll
+        for (int rr = 0; rr < kDR; ++rr) {
+            double sv = 0.0;
+            if (lane < wi) {
+                for (int o = 0; o < wout; ++o) sv += dcur[rr * kDS + o] * W[(size_t)o * wi + lane];
+                sv *= act_d(m.act[l - 1], cb(l - 1)[rr * kDS + lane], yb(l - 1)[rr * kDS + lane]);
+            }
+            dnext[rr * kDS + lane] = sv;  // zero beyond the layer's width: padding of the last GEMM
+        }
+        __syncwarp();
+        double* t = dcur;
+        dcur = dnext;
+        dnext = t;
+    }
+    // dE/dG = delta_1 W1: C[8 x nin] = A[8 x 32] B[32 x nin] on the tensor cores
+    double afr[kDH / 4];
+#pragma unroll
+    for (int ks = 0; ks < kDH / 4; ++ks) afr[ks] = dcur[r * kDS + 4 * ks + q];
+    const int ksteps = (H1 + 3) / 4;
+    for (int n0 = 0; n0 < nin; n0 += 8) {
+        double c2[2] = {0.0, 0.0};
+        const int n = n0 + r;  // B[k][n] = W1[k][n]
+#pragma unroll
+        for (int ks = 0; ks < kDH / 4; ++ks) {
+            if (ks < ksteps) {
+                const int k = 4 * ks + q;
+                const double bb = (k < H1 && n < nin) ? W1[(size_t)k * nin + n] : 0.0;
+                dmma(c2, afr[ks], bb);
+            }
+        }
+        if (atom >= 0)
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                const int col = n0 + 2 * q + v;
+                if (col < nin) b.dEdG[(size_t)atom * nsf + col] = c2[v];
+            }
+    }
+}
+
+// The tensor-core form takes networks whose layers are at most kDH wide,
+// with one output and at most 8 layers.
+bool dmma_fits(const DevModel& m) {
+    if (m.nlayers < 1 || m.nlayers > 8 || m.width[m.nlayers] != 1) return false;
+    for (int l = 1; l <= m.nlayers; ++l)
+        if (m.width[l] > kDH) return false;
+    return true;
+}
+
 }  // namespace
 
 int launch_element_groups(const Batch& b, const DevModel& m, cudaStream_t s) {
@@ -107,7 +278,14 @@ void run_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
 }
 
 int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
-    run_mlp<double>(b, m, s);
+    if (!dmma_fits(m)) {
+        run_mlp<double>(b, m, s);
+        return 1;
+    }
+    const size_t smem = (size_t)dmma_warp_doubles(m.nlayers) * sizeof(double) * kDW;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_mlp_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const long long warps = b.natoms / kDR + m.nel + 1;  // >= the tiles of all elements
+    k_mlp_dmma<<<(unsigned)((warps + kDW - 1) / kDW), 32 * kDW, smem, s>>>(b, m);
     return 1;
 }
 
