@@ -1264,8 +1264,9 @@ int hdnnp_calc_neighbor_lists(hdnnp_ctx* c, int nat, const int32_t* Z, const dou
 
 // The lists of the last hdnnp_calc_neighbor_lists in the reference's
 // neighborList layout (neighborLists.f90:10-16): per atom nNeis = count + 1
-// entries, entry 1 the atom itself at its wrapped position, then its
-// neighbours (index, Cartesian image position) in list order.
+// entries, entry 1 the atom itself (a cell's atoms at their wrapped
+// positions, a molecule's where they were given), then its neighbours
+// (index, Cartesian image position in the frame of the input) in list order.
 int hdnnp_neighbor_lists_fetch(hdnnp_ctx* c, int* nneis, int* ineis, double* neis) {
     if (!c || !nneis) return fail(HDNNP_E_INPUT, "null argument");
     if (c->stage_seq < 1) return fail(HDNNP_E_STATE, "no lists: call hdnnp_calc_neighbor_lists first");
@@ -1291,7 +1292,7 @@ int hdnnp_neighbor_lists_fetch(hdnnp_ctx* c, int* nneis, int* ineis, double* nei
     for (int i = 0; i < nat; ++i) {
         if (ineis) ineis[o] = i;
         if (neis)
-            for (int d = 0; d < 3; ++d) neis[3 * o + d] = w[3 * (size_t)i + d];
+            for (int d = 0; d < 3; ++d) neis[3 * o + d] = w[3 * (size_t)i + d] + S.org[d];
         ++o;
         for (int q = off[i]; q < off[i + 1]; ++q, ++o) {
             const int j = nj[q];
@@ -1306,7 +1307,8 @@ int hdnnp_neighbor_lists_fetch(hdnnp_ctx* c, int* nneis, int* ineis, double* nei
                 if (sy) l[d] += S.h[3 + d] * sy;
                 if (sx) l[d] += S.h[0 + d] * sx;
             }
-            for (int d = 0; d < 3; ++d) neis[3 * o + d] = w[3 * (size_t)j + d] + l[d];
+            // a molecule's box origin added back (neighborLists.f90:217)
+            for (int d = 0; d < 3; ++d) neis[3 * o + d] = (w[3 * (size_t)j + d] + l[d]) + S.org[d];
         }
     }
     return HDNNP_OK;

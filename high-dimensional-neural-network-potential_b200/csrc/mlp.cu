@@ -91,12 +91,14 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double bb) {
 constexpr int kDW = 4;   // warps per block
 constexpr int kDH = 32;  // widest layer the kernel takes
 constexpr int kDR = 8;   // atoms per warp
-constexpr int kDS = kDH + 1;  // row stride of the per-warp activation rows
 
-// per warp: c_l and y_l of every layer and two delta buffers, [8][kDS] each
-__host__ __device__ inline int dmma_warp_doubles(int L) { return (2 * L + 2) * kDR * kDS; }
+// Row stride of the per-warp activation rows: the widest layer + 1, odd.
+__host__ __device__ inline int dmma_stride(int maxw) { return (maxw + 1) | 1; }
+// per warp: act'(c_l) of every layer and two rotating rows (activations in
+// the forward pass, deltas in the backward pass), [8][stride] each
+__host__ __device__ inline int dmma_warp_doubles(int L, int stride) { return (L + 2) * kDR * stride; }
 
-__global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
+__global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int S) {
     extern __shared__ __align__(16) double dsm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int L = m.nlayers;
@@ -114,12 +116,9 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
         tile -= nt;
     }
     if (e < 0) return;  // uniform per warp
-    double* ws = dsm + (size_t)wib * dmma_warp_doubles(L);
-    // c_l and y_l of layer l (0-based)
-    auto cb = [&](int l) { return ws + (2 * l) * kDR * kDS; };
-    auto yb = [&](int l) { return ws + (2 * l + 1) * kDR * kDS; };
-    double* dcur = ws + (2 * L) * kDR * kDS;
-    double* dnext = dcur + kDR * kDS;
+    double* ws = dsm + (size_t)wib * dmma_warp_doubles(L, S);
+    auto da = [&](int l) { return ws + l * kDR * S; };          // act'(c_l)
+    auto yb = [&](int p) { return ws + (L + p) * kDR * S; };    // rotating rows
     const int r = lane >> 2, q = lane & 3;
     const int atom = r < cnt ? b.el_atoms[t0 + r] : -1;
     const int nin = m.nin_el[e], nsf = m.nsf_max, H1 = m.width[1];
@@ -130,6 +129,7 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
     const double* grow = atom >= 0 ? b.G + (size_t)atom * nsf : nullptr;
+#pragma unroll 4
     for (int k0 = 0; k0 < nin; k0 += 4) {
         const int k = k0 + q;
         const double a = (grow && k < nin) ? grow[k] : 0.0;
@@ -147,13 +147,12 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
                 const int col = nt * 8 + 2 * q + v;
-                double cv = 0.0, yv = 0.0;
                 if (col < H1) {
-                    cv = acc[nt][v] + b1[col];
-                    yv = act_f(m.act[0], cv);
+                    const double cv = acc[nt][v] + b1[col];
+                    const double yv = act_f(m.act[0], cv);
+                    yb(0)[r * S + col] = yv;
+                    da(0)[r * S + col] = act_d(m.act[0], cv, yv);
                 }
-                cb(0)[r * kDS + col] = cv;
-                yb(0)[r * kDS + col] = yv;
             }
     }
     __syncwarp();
@@ -162,6 +161,8 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
         const int win = m.width[l], wout = m.width[l + 1];
         const double* W = m.w + m.w_off[e * L + l];  // [wout][win]
         const double* bl = m.b + m.b_off[e * L + l];
+        const double* yin = yb((l - 1) & 1);
+        double* yout = yb(l & 1);
         if (lane < wout) {
             double sacc[kDR];
 #pragma unroll
@@ -169,40 +170,40 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
             for (int i = 0; i < win; ++i) {
                 const double w = W[(size_t)lane * win + i];
 #pragma unroll
-                for (int rr = 0; rr < kDR; ++rr) sacc[rr] += w * yb(l - 1)[rr * kDS + i];
+                for (int rr = 0; rr < kDR; ++rr) sacc[rr] += w * yin[rr * S + i];
             }
 #pragma unroll
             for (int rr = 0; rr < kDR; ++rr) {
                 const double cv = sacc[rr] + bl[lane];
-                cb(l)[rr * kDS + lane] = cv;
-                yb(l)[rr * kDS + lane] = act_f(m.act[l], cv);
+                const double yv = act_f(m.act[l], cv);
+                yout[rr * S + lane] = yv;
+                da(l)[rr * S + lane] = act_d(m.act[l], cv, yv);
             }
         }
         __syncwarp();
     }
-    // atomic energies
-    if (lane < cnt) b.atE[b.el_atoms[t0 + lane]] = yb(L - 1)[lane * kDS] + m.atom_energy[e];
-    // backward: delta of the output layer (gradOut = 1), then down to layer 1
+    // atomic energies, then the rotating rows carry the deltas
+    if (lane < cnt) b.atE[b.el_atoms[t0 + lane]] = yb((L - 1) & 1)[lane * S] + m.atom_energy[e];
+    __syncwarp();
+    double* dcur = yb(0);
+    double* dnext = yb(1);
     {
-        const int w = m.width[L];
+        const int w = m.width[L];  // gradOut = 1
         if (lane < w)
 #pragma unroll
-            for (int rr = 0; rr < kDR; ++rr)
-                dcur[rr * kDS + lane] = act_d(m.act[L - 1], cb(L - 1)[rr * kDS + lane], yb(L - 1)[rr * kDS + lane]);
+            for (int rr = 0; rr < kDR; ++rr) dcur[rr * S + lane] = da(L - 1)[rr * S + lane];
     }
     __syncwarp();
     for (int l = L - 1; l >= 1; --l) {
         const int wout = m.width[l + 1], wi = m.width[l];
         const double* W = m.w + m.w_off[e * L + l];  // [wout][wi]
+        if (lane < wi)
 #pragma unroll
-        for (int rr = 0; rr < kDR; ++rr) {
-            double sv = 0.0;
-            if (lane < wi) {
-                for (int o = 0; o < wout; ++o) sv += dcur[rr * kDS + o] * W[(size_t)o * wi + lane];
-                sv *= act_d(m.act[l - 1], cb(l - 1)[rr * kDS + lane], yb(l - 1)[rr * kDS + lane]);
+            for (int rr = 0; rr < kDR; ++rr) {
+                double sv = 0.0;
+                for (int o = 0; o < wout; ++o) sv += dcur[rr * S + o] * W[(size_t)o * wi + lane];
+                dnext[rr * S + lane] = sv * da(l - 1)[rr * S + lane];
             }
-            dnext[rr * kDS + lane] = sv;  // zero beyond the layer's width: padding of the last GEMM
-        }
         __syncwarp();
         double* t = dcur;
         dcur = dnext;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m) {
     // dE/dG = delta_1 W1: C[8 x nin] = A[8 x 32] B[32 x nin] on the tensor cores
     double afr[kDH / 4];
 #pragma unroll
-    for (int ks = 0; ks < kDH / 4; ++ks) afr[ks] = dcur[r * kDS + 4 * ks + q];
+    for (int ks = 0; ks < kDH / 4; ++ks) afr[ks] = (4 * ks + q < H1) ? dcur[r * S + 4 * ks + q] : 0.0;
     const int ksteps = (H1 + 3) / 4;
     for (int n0 = 0; n0 < nin; n0 += 8) {
         double c2[2] = {0.0, 0.0};
@@ -282,10 +283,13 @@ int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
         run_mlp<double>(b, m, s);
         return 1;
     }
-    const size_t smem = (size_t)dmma_warp_doubles(m.nlayers) * sizeof(double) * kDW;
+    int maxw = 1;
+    for (int l = 1; l <= m.nlayers; ++l) maxw = maxw > m.width[l] ? maxw : m.width[l];
+    const int S = dmma_stride(maxw);
+    const size_t smem = (size_t)dmma_warp_doubles(m.nlayers, S) * sizeof(double) * kDW;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_mlp_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const long long warps = b.natoms / kDR + m.nel + 1;  // >= the tiles of all elements
-    k_mlp_dmma<<<(unsigned)((warps + kDW - 1) / kDW), 32 * kDW, smem, s>>>(b, m);
+    k_mlp_dmma<<<(unsigned)((warps + kDW - 1) / kDW), 32 * kDW, smem, s>>>(b, m, S);
     return 1;
 }
 
