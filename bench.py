@@ -476,6 +476,26 @@ def leg_c1(W, engine, PLm, timed):
         E, F, _ = pot1.energy_and_forces(engine.AtStruct(s["Z"], x))
         p = p + 10.0 * (F + Fl)
     hsec = time.perf_counter() - t0
+    # the plain call alone: through the Python wrapper, and straight through
+    # the C ABI with preallocated host buffers (the reference's call shape)
+    ncall = 2000
+    t0 = time.perf_counter()
+    for _ in range(ncall):
+        pot1.energy_and_forces(ats)
+    wsec = (time.perf_counter() - t0) / ncall
+    L = engine.lib()
+    Zc = np.ascontiguousarray(s["Z"], np.int32)
+    Xc = np.ascontiguousarray(s["pos"], np.float64)
+    Ec, Fc = C.c_double(), np.zeros((len(Zc), 3))
+    args = (pot1._c, len(Zc), Zc.ctypes.data_as(C.POINTER(C.c_int)),
+            Xc.ctypes.data_as(C.POINTER(C.c_double)), 0, None, C.byref(Ec),
+            Fc.ctypes.data_as(C.POINTER(C.c_double)), None)
+    for _ in range(100):
+        L.hdnnp_energy_and_forces(*args)
+    t0 = time.perf_counter()
+    for _ in range(ncall):
+        L.hdnnp_energy_and_forces(*args)
+    csec = (time.perf_counter() - t0) / ncall
     # CPU stand-in: the oracle (all host threads) running the same MD loop
     from oracle import oracle as O
 
@@ -496,6 +516,9 @@ def leg_c1(W, engine, PLm, timed):
         "kernels_per_step": pl.info()["kernels_per_launch"] / 100,
         "graph_us_per_step": gsec / 1000 * 1e6, "graph_kernels_per_step": g_kernels,
         "plain_api_steps_per_s": nh / hsec, "plain_api_us_per_step": hsec / nh * 1e6,
+        "plain_call_us": {"python_wrapper": wsec * 1e6, "c_abi": csec * 1e6,
+                          "what": "one hdnnp_energy_and_forces on the 8-atom molecule, host arrays in and out, "
+                                  "mean of 2000 back-to-back calls"},
         "cpu_oracle_steps_per_s": 1000 / csec, "cpu_cores": O.max_threads()}
     pl.close()
     pot1.close()

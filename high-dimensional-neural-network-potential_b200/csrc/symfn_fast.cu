@@ -963,7 +963,9 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
 }
 
 template <typename T, class S>
-__global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 4) k_sfg_fast(Batch b, DevModel m, int mm, int mlo, int last) {
+// FP64: 5 blocks per SM at 96 registers (a few spills) beat 4 at 120 (23.1
+// against 23.9 ms on the C4 batch); the value pass loses at 5 (27.4 against 24.6)
+__global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 5) k_sfg_fast(Batch b, DevModel m, int mm, int mlo, int last) {
     constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
