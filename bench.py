@@ -495,7 +495,7 @@ def leg_c1(W, engine, PLm, timed):
     t0 = time.perf_counter()
     for _ in range(ncall):
         L.hdnnp_energy_and_forces(*args)
-    csec = (time.perf_counter() - t0) / ncall
+    asec = (time.perf_counter() - t0) / ncall
     # CPU stand-in: the oracle (all host threads) running the same MD loop
     from oracle import oracle as O
 
@@ -516,7 +516,7 @@ def leg_c1(W, engine, PLm, timed):
         "kernels_per_step": pl.info()["kernels_per_launch"] / 100,
         "graph_us_per_step": gsec / 1000 * 1e6, "graph_kernels_per_step": g_kernels,
         "plain_api_steps_per_s": nh / hsec, "plain_api_us_per_step": hsec / nh * 1e6,
-        "plain_call_us": {"python_wrapper": wsec * 1e6, "c_abi": csec * 1e6,
+        "plain_call_us": {"python_wrapper": wsec * 1e6, "c_abi": asec * 1e6,
                           "what": "one hdnnp_energy_and_forces on the 8-atom molecule, host arrays in and out, "
                                   "mean of 2000 back-to-back calls"},
         "cpu_oracle_steps_per_s": 1000 / csec, "cpu_cores": O.max_threads()}

@@ -520,9 +520,39 @@ int upload_model(hdnnp_model* m) {
             tcb.assign(8, 0);
         }
     }
+    // First layer in the register-fragment order of the FP64 tensor-core
+    // network kernel (mma m8n8k4 f64: lane t holds B[t % 4][t / 4]); each
+    // fragment is one coalesced 256-byte load.
+    std::vector<double> dmf, dmb;
+    {
+        bool ok = L >= 1 && L <= 8 && D.width[L] == 1;
+        for (int l = 1; l <= L && ok; ++l) ok = D.width[l] <= 32;
+        D.dm_ok = ok ? 1 : 0;
+        for (int c = 0; c < nel && ok; ++c) {
+            const Layer& l0 = H.el[c].net[0];
+            const int nin = l0.nin, H1 = l0.nout, KS = (nin + 3) / 4, NB = (nin + 7) / 8, KB = (H1 + 3) / 4;
+            D.dm_off_f[c] = (long long)dmf.size();
+            D.dm_off_b[c] = (long long)dmb.size();
+            for (int ks = 0; ks < KS; ++ks)
+                for (int nt = 0; nt < 4; ++nt)
+                    for (int t = 0; t < 32; ++t) {
+                        const int n = nt * 8 + t / 4, k = 4 * ks + t % 4;  // B[k][n] = W1[n][k]
+                        dmf.push_back(n < H1 && k < nin ? l0.w[(size_t)n * nin + k] : 0.0);
+                    }
+            for (int nb = 0; nb < NB; ++nb)
+                for (int ks = 0; ks < KB; ++ks)
+                    for (int t = 0; t < 32; ++t) {
+                        const int k = 4 * ks + t % 4, n = nb * 8 + t / 4;  // B[k][n] = W1[k][n]
+                        dmb.push_back(k < H1 && n < nin ? l0.w[(size_t)k * nin + n] : 0.0);
+                    }
+        }
+        if (dmf.empty()) dmf.assign(1, 0.0);
+        if (dmb.empty()) dmb.assign(1, 0.0);
+    }
     size_t o_pm = add(pmap.data(), pmap.size() * sizeof(short)), o_wf = add(wf.data(), wf.size() * 4),
            o_wtf = add(wtf.data(), wtf.size() * 4), o_bf = add(bf.data(), bf.size() * 4),
-           o_tcf = add(tcf.data(), tcf.size() * 2), o_tcb = add(tcb.data(), tcb.size() * 2);
+           o_tcf = add(tcf.data(), tcf.size() * 2), o_tcb = add(tcb.data(), tcb.size() * 2),
+           o_dmf = add(dmf.data(), dmf.size() * 8), o_dmb = add(dmb.data(), dmb.size() * 8);
     CUDA_TRY(cudaSetDevice(m->device));
     CUDA_TRY(cudaMalloc(&m->dmem, off));
     char* base = (char*)m->dmem;
@@ -558,6 +588,8 @@ int upload_model(hdnnp_model* m) {
     D.bf = (const float*)(base + o_bf);
     D.tc_fwd = (const unsigned short*)(base + o_tcf);
     D.tc_bwd = (const unsigned short*)(base + o_tcb);
+    D.dm_fwd = (const double*)(base + o_dmf);
+    D.dm_bwd = (const double*)(base + o_dmb);
     return HDNNP_OK;
 }
 

@@ -114,6 +114,16 @@ struct DevModel {
     float tc_inv_s1[kMaxEl];      // 1 / s1 per element
     const unsigned short* tc_fwd;
     const unsigned short* tc_bwd;
+    // First layer in the register-fragment order of the FP64 tensor-core
+    // network kernel (mma m8n8k4 f64, mlp.cu), zero-padded: forward
+    // B[k][n] = W1[n][k] as [ceil(nin/4)][4 n-tiles][32 lanes], input
+    // gradient B[k][n] = W1[k][n] as [ceil(nin/8)][ceil(H1/4)][32 lanes];
+    // per-element offsets in doubles.  dm_ok = 0 if the network does not fit.
+    int dm_ok;
+    long long dm_off_f[kMaxEl];
+    long long dm_off_b[kMaxEl];
+    const double* dm_fwd;
+    const double* dm_bwd;
 };
 
 // Workspace pointers for one batch evaluation (all device memory).

@@ -122,23 +122,33 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
     const int r = lane >> 2, q = lane & 3;
     const int atom = r < cnt ? b.el_atoms[t0 + r] : -1;
     const int nin = m.nin_el[e], nsf = m.nsf_max, H1 = m.width[1];
-    const double* W1 = m.w + m.w_off[e * L];  // [H1][nin]
-
-    // layer 1: C[8 x 32] = G[8 x nin] W1^T on the tensor cores
+    // layer 1: C[8 x 32] = G[8 x nin] W1^T on the tensor cores; the next
+    // k-step's operands are loaded while this one multiplies
     double acc[4][2];
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
     const double* grow = atom >= 0 ? b.G + (size_t)atom * nsf : nullptr;
-#pragma unroll 4
-    for (int k0 = 0; k0 < nin; k0 += 4) {
-        const int k = k0 + q;
-        const double a = (grow && k < nin) ? grow[k] : 0.0;
+    const double* F = m.dm_fwd + m.dm_off_f[e] + lane;  // [ks][nt][32]
+    const int KS = (nin + 3) >> 2;
+    double a_n = (grow && q < nin) ? __ldg(grow + q) : 0.0;
+    double b_n[4];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int n = nt * 8 + r;  // B[k][n] = W1[n][k]
-            const double bb = (n < H1 && k < nin) ? W1[(size_t)n * nin + k] : 0.0;
-            dmma(acc[nt], a, bb);
+    for (int nt = 0; nt < 4; ++nt) b_n[nt] = __ldg(F + nt * 32);
+#pragma unroll 2
+    for (int ks = 0; ks < KS; ++ks) {
+        const double a = a_n;
+        double bb[4];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) bb[nt] = b_n[nt];
+        if (ks + 1 < KS) {
+            const int k = 4 * (ks + 1) + q;
+            a_n = (grow && k < nin) ? __ldg(grow + k) : 0.0;
+            const double* f = F + (size_t)(ks + 1) * 128;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) b_n[nt] = __ldg(f + nt * 32);
         }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma(acc[nt], a, bb[nt]);
     }
     {
         const double* b1 = m.b + m.b_off[e * L];
@@ -213,34 +223,31 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
     double afr[kDH / 4];
 #pragma unroll
     for (int ks = 0; ks < kDH / 4; ++ks) afr[ks] = (4 * ks + q < H1) ? dcur[r * S + 4 * ks + q] : 0.0;
-    const int ksteps = (H1 + 3) / 4;
-    for (int n0 = 0; n0 < nin; n0 += 8) {
-        double c2[2] = {0.0, 0.0};
-        const int n = n0 + r;  // B[k][n] = W1[k][n]
+    // two n-tiles per iteration (independent accumulator chains)
+    const double* Bw = m.dm_bwd + m.dm_off_b[e] + lane;  // [nb][ks][32]
+    const int KB = (H1 + 3) >> 2, NB = (nin + 7) >> 3;
+    for (int nb = 0; nb < NB; nb += 2) {
+        const bool two = nb + 1 < NB;  // uniform
+        const double* b0 = Bw + (size_t)nb * KB * 32;
+        const double* b1 = b0 + KB * 32;
+        double c0[2] = {0.0, 0.0}, c1[2] = {0.0, 0.0};
 #pragma unroll
         for (int ks = 0; ks < kDH / 4; ++ks) {
-            if (ks < ksteps) {
-                const int k = 4 * ks + q;
-                const double bb = (k < H1 && n < nin) ? W1[(size_t)k * nin + n] : 0.0;
-                dmma(c2, afr[ks], bb);
+            if (ks < KB) {
+                dmma(c0, afr[ks], __ldg(b0 + ks * 32));
+                if (two) dmma(c1, afr[ks], __ldg(b1 + ks * 32));
             }
         }
-        if (atom >= 0)
+        if (atom >= 0) {
+            double* drow = b.dEdG + (size_t)atom * nsf;
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
-                const int col = n0 + 2 * q + v;
-                if (col < nin) b.dEdG[(size_t)atom * nsf + col] = c2[v];
+                const int col = nb * 8 + 2 * q + v;
+                if (col < nin) drow[col] = c0[v];
+                if (two && col + 8 < nin) drow[col + 8] = c1[v];
             }
+        }
     }
-}
-
-// The tensor-core form takes networks whose layers are at most kDH wide,
-// with one output and at most 8 layers.
-bool dmma_fits(const DevModel& m) {
-    if (m.nlayers < 1 || m.nlayers > 8 || m.width[m.nlayers] != 1) return false;
-    for (int l = 1; l <= m.nlayers; ++l)
-        if (m.width[l] > kDH) return false;
-    return true;
 }
 
 }  // namespace
@@ -278,8 +285,11 @@ void run_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
     k_mlp<T><<<tiles, kThreads, smem, s>>>(b, m, maxw);
 }
 
+// The tensor-core form takes networks whose layers are at most kDH wide,
+// with one output and at most 8 layers (dm_ok, set with the fragments at
+// model upload).
 int launch_mlp(const Batch& b, const DevModel& m, cudaStream_t s) {
-    if (!dmma_fits(m)) {
+    if (!m.dm_ok) {
         run_mlp<double>(b, m, s);
         return 1;
     }
