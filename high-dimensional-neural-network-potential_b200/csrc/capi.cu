@@ -563,13 +563,6 @@ int upload_model(hdnnp_model* m) {
     D.g2_off = (const int*)(base + o_g2o);
     D.g2max = 0;
     for (int c = 0; c < nel; ++c) D.g2max = std::max(D.g2max, g2_off[(size_t)c * nel + nel] - g2_off[(size_t)c * nel]);
-    {
-        int n2 = 1;
-        for (int q = 0; q < nel * nel; ++q) n2 = std::max(n2, g2_off[q + 1] - g2_off[q]);
-        int qq = 1;
-        while (qq < n2) qq <<= 1;
-        D.g2q = qq <= 32 ? qq : 0;
-    }
     D.g2 = (const SF2*)(base + o_g2);
     D.g4_off = (const int*)(base + o_g4o);
     D.g4 = (const SF4*)(base + o_g4);

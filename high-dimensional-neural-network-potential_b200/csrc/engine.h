@@ -63,8 +63,6 @@ struct DevModel {
     const int* nsf;           // [nel]
     const int* g2_off;        // [nel*nel+1]
     int g2max;                // most radial SFs of one centre element
-    int g2q;                  // power of two >= the most radial SFs of one (centre, neighbour) element
-                              // pair, if <= 32 (fast value pass: a lane per (neighbour, SF)), else 0
     const SF2* g2;
     const int* g4_off;        // [nel*nblk+1]
     const SF4* g4;
