@@ -206,10 +206,11 @@ struct hdnnp_ctx {
     // One molecule of at most kSmallMolecule atoms per call in FP64: the
     // single-block kernel of fused_md.cu in evaluation mode (option
     // "small_eval", default on).  se_dev: the io block (see small_eval_io)
-    // and the kernel's global homes; se_host: its pinned mirror.
+    // and the kernel's global homes; se_host: its mapped pinned mirror.
     int small_eval = 1;
     void* se_dev = nullptr;
     unsigned char* se_host = nullptr;
+    unsigned char* se_hdev = nullptr;  // device address of the mapped se_host
     Batch se_b{};
     // profiling: events around each stage, accumulated stage times and counters
     bool profile = false;
@@ -906,8 +907,9 @@ int small_eval_setup(hdnnp_ctx* c) {
     const size_t nd = 2 * N * nsf + 3 * NN + 9 * N, ni = 3 * NN;
     const size_t bytes = SmallEvalIo::homes + nd * 8 + ni * 4;
     CUDA_TRY(cudaMalloc(&c->se_dev, bytes));
-    CUDA_TRY(cudaMallocHost(&c->se_host, SmallEvalIo::homes));
+    CUDA_TRY(cudaHostAlloc((void**)&c->se_host, SmallEvalIo::homes, cudaHostAllocMapped));
     std::memset(c->se_host, 0, SmallEvalIo::homes);
+    CUDA_TRY(cudaHostGetDevicePointer((void**)&c->se_hdev, c->se_host, 0));
     unsigned char* base = (unsigned char*)c->se_dev;
     double* d = (double*)(base + SmallEvalIo::homes);
     int* q = (int*)(d + nd);
@@ -931,8 +933,9 @@ int small_eval_setup(hdnnp_ctx* c) {
 }
 
 // One molecule of nat <= kSmallMolecule atoms in FP64 through the
-// single-block kernel (fused_md.cu, evaluation mode): one host-to-device
-// copy, one kernel, one device-to-host copy, one wait.  Z must be validated.
+// single-block kernel (fused_md.cu, evaluation mode): one kernel and one
+// wait (plus a host-to-device and a device-to-host copy when the
+// warp-per-atom form runs).  Z must be validated.
 int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, double* energy, double* force) {
     int r;
     if ((r = small_eval_setup(c))) return r;
@@ -945,8 +948,18 @@ int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, doubl
     int* hacc = (int*)(h + SmallEvalIo::acc);
     hacc[0] = hacc[1] = 0;
     cudaStream_t st = c->stream;
-    CUDA_TRY(cudaMemcpyAsync(dv, h, SmallEvalIo::in_bytes, cudaMemcpyHostToDevice, st));
     Batch b = c->se_b;
+    // The item-parallel form reads its inputs once and writes its results
+    // once: it takes them straight from the mapped host block (no copies).
+    // The warp-per-atom form reads the element indices throughout and gets
+    // device copies.
+    const bool mapped = small_md_tiny(D, nat);
+    if (mapped) {
+        dv = c->se_hdev;
+        b.elem = (int*)(dv + SmallEvalIo::elem);
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(dv, h, SmallEvalIo::in_bytes, cudaMemcpyHostToDevice, st));
+    }
     b.natoms = nat;
     b.mmax = nat - 1;
     b.nentries = nat * nat;
@@ -962,7 +975,8 @@ int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, doubl
     launch_small_md(b, D, a, st);
     CUDA_TRY(cudaGetLastError());
     const size_t out = SmallEvalIo::force + sizeof(double) * 3 * nat - SmallEvalIo::out_off;
-    CUDA_TRY(cudaMemcpyAsync(h + SmallEvalIo::out_off, dv + SmallEvalIo::out_off, out, cudaMemcpyDeviceToHost, st));
+    if (!mapped)
+        CUDA_TRY(cudaMemcpyAsync(h + SmallEvalIo::out_off, dv + SmallEvalIo::out_off, out, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     c->launches = 1;
     c->have_last = false;  // the intermediates are not in the context's arrays

@@ -320,6 +320,9 @@ size_t mlp_tc_smem_bytes(const DevModel& m);
 size_t sf_smem_per_warp(int mmax, bool grad);
 int device_sm_count();  // multiprocessors of the current device (cached per device)
 size_t small_md_smem_bytes(const DevModel& m, int natoms);  // dynamic shared memory of the kernel
+// true when the item-parallel form runs: it reads its inputs once into
+// shared memory and writes its outputs once (host-mapped buffers are fine)
+bool small_md_tiny(const DevModel& m, int natoms);
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& a, cudaStream_t s);
 
 // Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).

@@ -836,6 +836,8 @@ size_t small_md_smem_bytes(const DevModel& m, int natoms) {
     return t != SIZE_MAX ? t : small_md_layout(m, natoms, nullptr);
 }
 
+bool small_md_tiny(const DevModel& m, int natoms) { return tiny_md_layout(m, natoms, nullptr) != SIZE_MAX; }
+
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& x, cudaStream_t s) {
     TinyArgs ta{};
     const size_t tsm = tiny_md_layout(m, x.natoms, &ta);

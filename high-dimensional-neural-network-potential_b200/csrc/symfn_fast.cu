@@ -45,7 +45,6 @@ template <typename T>
 struct FSmem {
     V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
     double4* dd;    // FP32 value pass: the FP64 relative vector (x, y, z, -) for the pair cutoff
-    float4* nf;     // FP64 value pass: the relative vector in FP32 for the pair pre-screen
     V4<T>* ax;      // fc, dfc/r, 1/r, -
     V4<T>* g;       // gradient accumulators (pass 2)
     int* ent;       // entry index of a slot (pass 2)
@@ -63,7 +62,6 @@ template <typename T>
 __host__ __device__ inline size_t fast_warp_bytes(int mm, int g2max, int nblk, int P, bool grad) {
     size_t b = a16(sizeof(V4<T>) * mm) * 2;
     if (sizeof(T) == 4 && !grad) b += a16(sizeof(double4) * mm);
-    if (sizeof(T) == 8 && !grad) b += a16(sizeof(float4) * mm);
     if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
     else b += a16(sizeof(T) * 32 * (P + 1));
     b += a16(mm) + 64 * sizeof(unsigned) + a16(sizeof(int) * (kMaxEl + 1)) + a16(sizeof(int) * kMaxEl);
@@ -80,7 +78,6 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int g2max, int nblk,
     };
     s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
     s.dd = (sizeof(T) == 4 && !grad) ? (double4*)take(sizeof(double4) * mm) : nullptr;
-    s.nf = (sizeof(T) == 8 && !grad) ? (float4*)take(sizeof(float4) * mm) : nullptr;
     s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
     if (grad) {
         s.g = (V4<T>*)take(sizeof(V4<T>) * mm);
@@ -302,8 +299,6 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
             s.nb[slot] = V4<T>{(T)dx, (T)dy, (T)dz, (T)r};
             if (sizeof(T) == 4 && s.dd)
                 s.dd[slot] = make_double4(dx, dy, dz, 0.0);
-            if (sizeof(T) == 8 && s.nf)
-                s.nf[slot] = make_float4((float)dx, (float)dy, (float)dz, 0.0f);
             s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)ir, (T)0};
             s.el[slot] = (unsigned char)el;
             if (kGrad) {
@@ -560,7 +555,6 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         const int Ms = fstage<T, false>(b, m, i, c, s, lane, M);
         const T rc = (T)m.rc[c], inv_rc = (T)(1.0 / m.rc[c]), rc2 = rc * rc;
         const double rc2d = m.rc[c] * m.rc[c];
-        const float rc2lo = (float)(rc2d * (1.0 - 1e-4)), rc2hi = (float)(rc2d * (1.0 + 1e-4));
         T* Gi = Gout + (size_t)i * m.nsf_max;
         const double* mean = m.smean + (size_t)c * m.nsf_max;
         const double* iwidth = m.sinvw + (size_t)c * m.nsf_max;
@@ -736,28 +730,10 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             n_cand += ncand;
             for (int cb = 0; cb < ncand; cb += 32) {
                 const int cidx = cb + lane;
-                bool ok = cidx < ncand, border = false;
+                bool ok = cidx < ncand;
                 int j = 0, k = 0;
                 if (ok) {
                     fpair(cidx, sa, na, sb, nb, same, inv_nb, j, k);
-                    if constexpr (sizeof(T) == 8) {
-                        // FP32 pre-screen of the FP64 test r_jk^2 < rc^2:
-                        // the FP32 vectors put r_jk^2 within ~1e-6 relative
-                        // of its FP64 value, so only candidates within 1e-4
-                        // of rc^2 (or non-finite) take the FP64 test below,
-                        // and every decision equals the FP64 one
-                        const float4 a = s.nf[j], bb = s.nf[k];
-                        const float ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
-                        const float r2 = ex * ex + ey * ey + ez * ez;
-                        ok = r2 < rc2lo;
-                        border = !ok && !(r2 > rc2hi);
-                    } else {
-                        const V4<T> a = s.nb[j], bb = s.nb[k];
-                        const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
-                        ok = ex * ex + ey * ey + ez * ez < rc2;
-                    }
-                }
-                if (sizeof(T) == 8 && __any_sync(kFull, border) && border) {
                     const V4<T> a = s.nb[j], bb = s.nb[k];
                     const T ex = bb.x - a.x, ey = bb.y - a.y, ez = bb.z - a.z;
                     ok = ex * ex + ey * ey + ez * ez < rc2;
