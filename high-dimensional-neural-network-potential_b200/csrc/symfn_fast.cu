@@ -41,12 +41,37 @@ struct alignas(4 * sizeof(T)) V4 {
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// A staged neighbour record (x, y, z, w).  FP64: 48-byte stride (16 bytes
+// of padding), so that the two 16-byte loads of random slots spread over all
+// 32 shared-memory banks; a 32-byte stride puts each load on 16 of them.
+template <typename T>
+struct SlotRec {
+    using type = V4<T>;
+};
+template <>
+struct SlotRec<double> {
+    struct alignas(16) type {
+        double x, y, z, w, p0, p1;
+        __device__ __forceinline__ operator V4<double>() const { return V4<double>{x, y, z, w}; }
+        __device__ __forceinline__ type& operator=(const V4<double>& v) {
+            x = v.x;
+            y = v.y;
+            z = v.z;
+            w = v.w;
+            return *this;
+        }
+    };
+};
+
 template <typename T>
 struct FSmem {
-    V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
+    using Rec = typename SlotRec<T>::type;
+    Rec* nb;        // dx, dy, dz, r        (centre - neighbour)
     double4* dd;    // FP32 value pass: the FP64 relative vector (x, y, z, -) for the pair cutoff
-    V4<T>* ax;      // fc, dfc/r, 1/r, -
-    V4<T>* g;       // gradient accumulators (pass 2)
+    Rec* ax;        // fc, dfc/r, 1/r, -
+    T* gx;          // gradient accumulators (pass 2), one array per component:
+    T* gy;          // a slot's x, y, z in one 16- or 32-byte record put random
+    T* gz;          // slots on 4 (FP64) or 8 (FP32) bank groups only
     int* ent;       // entry index of a slot (pass 2)
     unsigned char* el;
     unsigned* queue;
@@ -60,9 +85,9 @@ struct FSmem {
 
 template <typename T>
 __host__ __device__ inline size_t fast_warp_bytes(int mm, int g2max, int nblk, int P, bool grad) {
-    size_t b = a16(sizeof(V4<T>) * mm) * 2;
+    size_t b = a16(sizeof(typename SlotRec<T>::type) * mm) * 2;
     if (sizeof(T) == 4 && !grad) b += a16(sizeof(double4) * mm);
-    if (grad) b += a16(sizeof(V4<T>) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
+    if (grad) b += 3 * a16(sizeof(T) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
     else b += a16(sizeof(T) * 32 * (P + 1));
     b += a16(mm) + 64 * sizeof(unsigned) + a16(sizeof(int) * (kMaxEl + 1)) + a16(sizeof(int) * kMaxEl);
     return b;
@@ -76,11 +101,13 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int g2max, int nblk,
         p += a16(bytes);
         return q;
     };
-    s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
+    s.nb = (typename FSmem<T>::Rec*)take(sizeof(typename FSmem<T>::Rec) * mm);
     s.dd = (sizeof(T) == 4 && !grad) ? (double4*)take(sizeof(double4) * mm) : nullptr;
-    s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
+    s.ax = (typename FSmem<T>::Rec*)take(sizeof(typename FSmem<T>::Rec) * mm);
     if (grad) {
-        s.g = (V4<T>*)take(sizeof(V4<T>) * mm);
+        s.gx = (T*)take(sizeof(T) * mm);
+        s.gy = (T*)take(sizeof(T) * mm);
+        s.gz = (T*)take(sizeof(T) * mm);
         s.ent = (int*)take(sizeof(int) * mm);
         s.w2 = (T*)take(sizeof(T) * g2max);
         s.WA = (T*)take(sizeof(T) * nblk * P);
@@ -302,7 +329,7 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
             s.ax[slot] = V4<T>{(T)fc, (T)dfc, (T)ir, (T)0};
             s.el[slot] = (unsigned char)el;
             if (kGrad) {
-                s.g[slot] = V4<T>{(T)0, (T)0, (T)0, (T)0};
+                s.gx[slot] = s.gy[slot] = s.gz[slot] = (T)0;
                 s.ent[slot] = e0 + q;
             }
         }
@@ -891,9 +918,9 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
             const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
             const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
-            atomicAdd(&s.g[pq].x, gkx);
-            atomicAdd(&s.g[pq].y, gky);
-            atomicAdd(&s.g[pq].z, gkz);
+            atomicAdd(&s.gx[pq], gkx);
+            atomicAdd(&s.gy[pq], gky);
+            atomicAdd(&s.gz[pq], gkz);
         }
         // Queue order is enumeration order, so pairs sharing j sit in
         // contiguous lanes: a segmented suffix sum (fixed shuffle order)
@@ -918,9 +945,9 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
                 }
             }
             if (head && lane < n) {
-                atomicAdd(&s.g[pj].x, gjx);
-                atomicAdd(&s.g[pj].y, gjy);
-                atomicAdd(&s.g[pj].z, gjz);
+                atomicAdd(&s.gx[pj], gjx);
+                atomicAdd(&s.gy[pj], gjy);
+                atomicAdd(&s.gz[pj], gjz);
             }
         }
 }
@@ -988,11 +1015,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 5) k_sfg_fas
                 const T e = xexp(-eta * xr * xr);
                 coef += s.w2[f - r0] * (-e * x.y + (T)2 * eta * xr * x.z * e * x.x);
             }
-            V4<T> g = s.g[t];
-            g.x += coef * d.x;
-            g.y += coef * d.y;
-            g.z += coef * d.z;
-            s.g[t] = g;
+            s.gx[t] += coef * d.x;
+            s.gy[t] += coef * d.y;
+            s.gz[t] += coef * d.z;
         }
         __syncwarp();
 
@@ -1054,7 +1079,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 5) k_sfg_fas
         T sx = 0, sy = 0, sz = 0;
         T v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (int t = lane; t < Ms; t += 32) {
-            const V4<T> g = s.g[t];
+            const V4<T> g{s.gx[t], s.gy[t], s.gz[t], (T)0};
             const V4<T> d = s.nb[t];
             const size_t e = (size_t)s.ent[t];
             gent[3 * e] = g.x;
