@@ -582,8 +582,6 @@ int upload_model(hdnnp_model* m) {
     D.bf = (const float*)(base + o_bf);
     D.tc_fwd = (const unsigned short*)(base + o_tcf);
     D.tc_bwd = (const unsigned short*)(base + o_tcb);
-    D.pf_base = base;
-    D.pf_bytes = (long long)o_pm;  // rc .. atom energies (added first)
     D.dm_fwd = (const double*)(base + o_dmf);
     D.dm_bwd = (const double*)(base + o_dmb);
     return HDNNP_OK;

@@ -122,11 +122,6 @@ struct DevModel {
     long long dm_off_b[kMaxEl];
     const double* dm_fwd;
     const double* dm_bwd;
-    // the FP64 tables above (SF records, scaling, weights), one contiguous
-    // range at the start of the model's device block: the single-block
-    // kernels prefetch it into L1
-    const char* pf_base;
-    long long pf_bytes;
 };
 
 // Workspace pointers for one batch evaluation (all device memory).

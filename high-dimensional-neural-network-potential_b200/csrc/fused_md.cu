@@ -125,14 +125,6 @@ __device__ __forceinline__ void mlp_rows(const Batch& b, const DevModel& m, int 
     }
 }
 
-// The model's FP64 tables into L1 at the start of a launch: every stage
-// reads them, and an evaluation-only launch would otherwise pay an L2
-// round trip for them in each stage.  Prefetches do not wait.
-__device__ __forceinline__ void prefetch_model(const DevModel& m, int tid, int nt) {
-    const long long lines = m.pf_bytes > 192 * 1024 ? 192 * 1024 / 128 : (m.pf_bytes + 127) / 128;
-    for (long long l = tid; l < lines; l += nt) asm volatile("prefetch.global.L1 [%0];" ::"l"(m.pf_base + l * 128));
-}
-
 template <int GM>
 __global__ void __launch_bounds__(kThreads, 1) k_small_md(Batch g, DevModel m, FusedArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -166,7 +158,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_small_md(Batch g, DevModel m, F
     b.info = info;
     b.wpos = pos;
     b.stats = nullptr;
-    prefetch_model(m, tid, blockDim.x);
     for (int q = tid; q < n3; q += blockDim.x) {
         pos[q] = a.pos[q];
         mom[q] = a.eval_only ? 0.0 : a.mom[q];
@@ -441,7 +432,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
     int* recblk = (int*)(smem + a.slot[tRecBlk]);    // block of each angular record
     int* blkof = (int*)(smem + a.slot[tBlkOf]);      // block of an element pair
     int* status = (int*)(smem + a.slot[tStatus]);
-    prefetch_model(m, tid, nt);
     for (int q = tid; q < n3; q += nt) {
         pos[q] = a.pos[q];
         mom[q] = a.eval_only ? 0.0 : a.mom[q];

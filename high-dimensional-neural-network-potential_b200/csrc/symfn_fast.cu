@@ -41,34 +41,11 @@ struct alignas(4 * sizeof(T)) V4 {
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// A staged neighbour record (x, y, z, w).  FP64: 48-byte stride (16 bytes
-// of padding), so that the two 16-byte loads of random slots spread over all
-// 32 shared-memory banks; a 32-byte stride puts each load on 16 of them.
-template <typename T>
-struct SlotRec {
-    using type = V4<T>;
-};
-template <>
-struct SlotRec<double> {
-    struct alignas(16) type {
-        double x, y, z, w, p0, p1;
-        __device__ __forceinline__ operator V4<double>() const { return V4<double>{x, y, z, w}; }
-        __device__ __forceinline__ type& operator=(const V4<double>& v) {
-            x = v.x;
-            y = v.y;
-            z = v.z;
-            w = v.w;
-            return *this;
-        }
-    };
-};
-
 template <typename T>
 struct FSmem {
-    using Rec = typename SlotRec<T>::type;
-    Rec* nb;        // dx, dy, dz, r        (centre - neighbour)
+    V4<T>* nb;      // dx, dy, dz, r        (centre - neighbour)
     double4* dd;    // FP32 value pass: the FP64 relative vector (x, y, z, -) for the pair cutoff
-    Rec* ax;        // fc, dfc/r, 1/r, -
+    V4<T>* ax;      // fc, dfc/r, 1/r, -
     T* gx;          // gradient accumulators (pass 2), one array per component:
     T* gy;          // a slot's x, y, z in one 16- or 32-byte record put random
     T* gz;          // slots on 4 (FP64) or 8 (FP32) bank groups only
@@ -85,7 +62,7 @@ struct FSmem {
 
 template <typename T>
 __host__ __device__ inline size_t fast_warp_bytes(int mm, int g2max, int nblk, int P, bool grad) {
-    size_t b = a16(sizeof(typename SlotRec<T>::type) * mm) * 2;
+    size_t b = a16(sizeof(V4<T>) * mm) * 2;
     if (sizeof(T) == 4 && !grad) b += a16(sizeof(double4) * mm);
     if (grad) b += 3 * a16(sizeof(T) * mm) + a16(sizeof(int) * mm) + a16(sizeof(T) * g2max) + 2 * a16(sizeof(T) * nblk * P);
     else b += a16(sizeof(T) * 32 * (P + 1));
@@ -101,9 +78,9 @@ __device__ inline FSmem<T> fcarve(unsigned char* p, int mm, int g2max, int nblk,
         p += a16(bytes);
         return q;
     };
-    s.nb = (typename FSmem<T>::Rec*)take(sizeof(typename FSmem<T>::Rec) * mm);
+    s.nb = (V4<T>*)take(sizeof(V4<T>) * mm);
     s.dd = (sizeof(T) == 4 && !grad) ? (double4*)take(sizeof(double4) * mm) : nullptr;
-    s.ax = (typename FSmem<T>::Rec*)take(sizeof(typename FSmem<T>::Rec) * mm);
+    s.ax = (V4<T>*)take(sizeof(V4<T>) * mm);
     if (grad) {
         s.gx = (T*)take(sizeof(T) * mm);
         s.gy = (T*)take(sizeof(T) * mm);
