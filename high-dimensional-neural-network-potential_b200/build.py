@@ -7,6 +7,7 @@ statically, so the library needs only the NVIDIA driver at run time.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -42,18 +43,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     objdir = os.path.join(HERE, "lib", "obj")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
     common = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
               "-I", os.path.join(ROOT, "include")]
-    for src in sources():
+
+    def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, *common, "-c", src, "-o", obj]
-        if src.endswith(".cu"):
-            cmd += ["-Xptxas", "-v"] if verbose else []
-        else:
-            cmd += ["-x", "cu"] if False else []
+        if src.endswith(".cu") and verbose:
+            cmd += ["-Xptxas", "-v"]
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        return obj
+
+    # one nvcc per source file, in parallel (the translation units are independent)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, sources()))
     subprocess.run([NVCC, *ARCH, "-shared", "-ccbin", HOST_CXX, "-o", LIB, *objs], check=True)
     return LIB
 

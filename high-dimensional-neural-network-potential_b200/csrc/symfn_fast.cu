@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "engine.h"
+#include "fastmath.cuh"
 
 namespace hdnnp {
 
@@ -128,15 +129,18 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-// precision-dispatched math
-__device__ __forceinline__ double xsqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
-// r and 1/r from r^2 > 0 by one reciprocal square root and a product: FP64
-// rsqrt (1 ulp), FP32 rsqrtf (2 ulp)
-__device__ __forceinline__ void dist_inv(double r2, double& r, double& ir) {
-    ir = rsqrt(r2);
-    r = r2 * ir;
+// precision-dispatched math.  FP64: the branch-free forms of fastmath.cuh
+// for the bounded arguments of these kernels (exp of -eta r^2, tanh of
+// u = 1 - r/rc in [0, 1], square roots of squared distances).
+__device__ __forceinline__ double xsqrt(double x) {
+    double r, ir;
+    sqrt_rsqrt(x, r, ir);
+    return r;
 }
+__device__ __forceinline__ float xsqrt(float x) { return sqrtf(x); }
+// r and 1/r from r^2 > 0: FP64 by the refined reciprocal square root of
+// fastmath.cuh, FP32 by rsqrtf (2 ulp) and a product
+__device__ __forceinline__ void dist_inv(double r2, double& r, double& ir) { sqrt_rsqrt(r2, r, ir); }
 __device__ __forceinline__ void dist_inv(float r2, float& r, float& ir) {
     ir = rsqrtf(r2);
     r = r2 * ir;
@@ -145,11 +149,12 @@ __device__ __forceinline__ void dist_inv(float r2, float& r, float& ir) {
 // b between 2^-126 and 2^126)
 __device__ __forceinline__ double xdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float xdiv(float a, float b) { return __fdividef(a, b); }
-__device__ __forceinline__ double xexp(double x) { return exp(x); }
+__device__ __forceinline__ double xexp(double x) { return exp_clamped(x); }
 // FP32 form: the exp2-based intrinsic (max error 2 + floor(1.173 |x|) ulp;
 // the angular arguments stay below ~5, where it is within 8 ulp)
 __device__ __forceinline__ float xexp(float x) { return __expf(x); }
-__device__ __forceinline__ double xtanh(double x) { return tanh(x); }
+// tanh of a cutoff argument u = 1 - r/rc in [0, 1]
+__device__ __forceinline__ double xtanh(double x) { return tanh01(x); }
 __device__ __forceinline__ float xtanh(float x) { return tanhf(x); }
 __device__ __forceinline__ double xpow(double x, double y) { return pow(x, y); }
 __device__ __forceinline__ float xpow(float x, float y) { return powf(x, y); }
@@ -291,12 +296,13 @@ __device__ int fstage(const Batch& b, const DevModel& m, int i, int c, FSmem<T>&
         }
         __syncwarp();
         if (keep) {
-            // distance and cutoff in FP64 (one division)
-            const double r = sqrt(dx * dx + dy * dy + dz * dz);
-            const double ir = 1.0 / r, irc = 1.0 / rc;
+            // distance and cutoff in FP64
+            double r, ir;
+            sqrt_rsqrt(dx * dx + dy * dy + dz * dz, r, ir);
+            const double irc = 1.0 / rc;
             double fc = 0.0, dfc = 0.0;
             if (r < rc) {
-                const double t = tanh(1.0 - r * irc), tt = t * t;
+                const double t = tanh01(1.0 - r * irc), tt = t * t;
                 fc = tt * t;
                 dfc = -3.0 * irc * ir * (tt - tt * tt);
             }
@@ -566,7 +572,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         // radial SFs: lane = SF, its neighbour element's staged neighbours in
         // order.  (A lane per (neighbour, SF) with shuffle sums was measured
         // slower in both precisions: 25.4 against 20.8 ms per C4 step in
-        // FP64, 14.9 against 12.8 in FP32.)
+        // FP64, 14.9 against 12.8 in FP32.  Groups of lanes per neighbour
+        // element, each lane a function and a share of the neighbours, with a
+        // butterfly over the groups, were slower too: 21.4 against 20.5.)
         const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
         for (int f = r0 + lane; f < r1; f += 32) {
             const SF2 q = m.g2[f];
@@ -802,6 +810,41 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
 }
 
 // ---------------------------------------------------------------- pass 2
+// (x, y, z) of every lane with `live` set added to gradient slot `slot`.  The
+// lanes naming one slot form a group (__match_any_sync); its lowest lane adds
+// the other members' values in ascending lane order (indexed shuffles, as many
+// rounds as the largest group has members) and writes the slot with one plain
+// read-modify-write, so no two lanes write one slot and the result does not
+// depend on timing.  (Shared-memory FP64 atomicAdd measured 5.6 ms of the 21 ms
+// FP64 gradient pass on the 4096-structure batch, against 0.3 ms for plain
+// read-modify-writes; rounds of an integer atomicMin that elect one lane per
+// slot cost as much as the atomics.)  Called by all lanes.
+template <typename T>
+__device__ __forceinline__ void group_add(const FSmem<T>& s, bool live, int slot, T x, T y, T z, int lane) {
+    const unsigned grp = __match_any_sync(kFull, live ? slot : -1 - lane);
+    const int most = __reduce_max_sync(kFull, __popc(grp));
+    const bool lead = live && (grp & lanemask_lt()) == 0;
+    unsigned rest = grp & ~(1u << lane);
+    T sx = x, sy = y, sz = z;
+    for (int r = 1; r < most; ++r) {
+        const int src = rest ? __ffs(rest) - 1 : lane;
+        const T ox = __shfl_sync(kFull, x, src);
+        const T oy = __shfl_sync(kFull, y, src);
+        const T oz = __shfl_sync(kFull, z, src);
+        if (rest) {
+            rest &= rest - 1;
+            sx += ox;
+            sy += oy;
+            sz += oz;
+        }
+    }
+    if (lead) {
+        s.gx[slot] += sx;
+        s.gy[slot] += sy;
+        s.gz[slot] += sz;
+    }
+}
+
 // Gradient contributions of up to 32 contributing pairs (one per lane; pk =
 // j | k << 10 | block << 20, live for lane < n): dE/dr_k added to slot k,
 // dE/dr_j summed over runs of equal j (lanes hold pairs in enumeration order,
@@ -810,13 +853,15 @@ template <typename T, class S>
 __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m, int ne, T rc, T inv_rc, double rc2d,
                                            unsigned pk_in, int n, int lane) {
     constexpr int NL = S::NL, NZ = S::NZ, NE = S::NE, P = S::P;
-        // dE/dr_j of this lane's pair, summed over runs of equal j below
-        int pj = -1 - lane;
-        T gjx = (T)0, gjy = (T)0, gjz = (T)0;
+        // dE/dr_j of this lane's pair (summed over runs of equal j below) and
+        // dE/dr_k
+        int pj = -1 - lane, pq = -1 - lane;
+        T gjx = (T)0, gjy = (T)0, gjz = (T)0, gkx = (T)0, gky = (T)0, gkz = (T)0;
         if (lane < n) {
             const unsigned pk = pk_in;
             pj = pk & 0x3ff;
-            const int pq = (pk >> 10) & 0x3ff, pt = pk >> 20;
+            pq = (pk >> 10) & 0x3ff;
+            const int pt = pk >> 20;
             const V4<T> a = s.nb[pj], bq = s.nb[pq];
             const V4<T> xa = s.ax[pj], xb = s.ax[pq];
             const T fj = xa.x, fk = xb.x, dfj = xa.y, dfk = xb.y;
@@ -892,13 +937,12 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             gjx = pj1 * cx - pj2 * a.x + B2 * (a.x - cx) + Cf * (t1 * bq.x + a.x * cj);
             gjy = pj1 * cy - pj2 * a.y + B2 * (a.y - cy) + Cf * (t1 * bq.y + a.y * cj);
             gjz = pj1 * cz - pj2 * a.z + B2 * (a.z - cz) + Cf * (t1 * bq.z + a.z * cj);
-            const T gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
-            const T gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
-            const T gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
-            atomicAdd(&s.gx[pq], gkx);
-            atomicAdd(&s.gy[pq], gky);
-            atomicAdd(&s.gz[pq], gkz);
+            gkx = -pk1 * cx - pk2 * bq.x + B2 * (bq.x + cx) + Cf * (t1 * a.x + bq.x * ck);
+            gky = -pk1 * cy - pk2 * bq.y + B2 * (bq.y + cy) + Cf * (t1 * a.y + bq.y * ck);
+            gkz = -pk1 * cz - pk2 * bq.z + B2 * (bq.z + cz) + Cf * (t1 * a.z + bq.z * ck);
         }
+        group_add(s, lane < n, pq, gkx, gky, gkz, lane);
+        __syncwarp();
         // Queue order is enumeration order, so pairs sharing j sit in
         // contiguous lanes: a segmented suffix sum (fixed shuffle order)
         // leaves each run's total in its first lane, which alone
@@ -910,8 +954,10 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const unsigned heads = __ballot_sync(kFull, head);
             const unsigned after = heads & ~((2u << lane) - 1u);  // heads above this lane
             const int last = after ? __ffs(after) - 2 : 31;        // last lane of my run
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
+            // doubling steps up to the longest run of the chunk (later steps
+            // would add nothing)
+            const int longest = __reduce_max_sync(kFull, head ? last - lane + 1 : 1);
+            for (int d = 1; d < longest; d <<= 1) {
                 const T ox = __shfl_down_sync(kFull, gjx, d);
                 const T oy = __shfl_down_sync(kFull, gjy, d);
                 const T oz = __shfl_down_sync(kFull, gjz, d);
@@ -921,11 +967,9 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
                     gjz += oz;
                 }
             }
-            if (head && lane < n) {
-                atomicAdd(&s.gx[pj], gjx);
-                atomicAdd(&s.gy[pj], gjy);
-                atomicAdd(&s.gz[pj], gjz);
-            }
+            // run totals into their slots (one block's runs name distinct
+            // slots; a chunk that spans two blocks can name one twice)
+            group_add(s, head && lane < n, pj, gjx, gjy, gjz, lane);
         }
 }
 
