@@ -225,7 +225,8 @@ LIST_BYTES = {"atoms": 28, "entries": 16}
 # this workload (191,160 atoms), scaled by the atoms of a step: the traffic of
 # these kernels is per atom (positions, neighbour entries, G / dE/dG rows,
 # pair lists), so it grows in proportion.
-TRAFFIC_PER_ATOM = {"mixed": {"sf_values": 706.5e6 / 191160, "sf_gradients": 842.5e6 / 191160}}
+TRAFFIC_PER_ATOM = {"mixed": {"sf_values": 706.5e6 / 191160, "sf_gradients": 842.5e6 / 191160},
+                    "fp64": {"sf_values": 903.737e6 / 191160, "sf_gradients": 1171.905e6 / 191160}}
 
 
 def kernel_flops(stage, counters, evals):
