@@ -949,10 +949,10 @@ int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, doubl
     hacc[0] = hacc[1] = 0;
     cudaStream_t st = c->stream;
     Batch b = c->se_b;
-    // The item-parallel form reads its inputs once and writes its results
-    // once: it takes them straight from the mapped host block (no copies).
-    // The warp-per-atom form reads the element indices throughout and gets
-    // device copies.
+    // The item-parallel form gets its inputs with the launch (kernel
+    // parameters) and writes its results once, straight into the mapped host
+    // block (no copies).  The warp-per-atom form reads the element indices
+    // throughout and gets device copies.
     const bool mapped = small_md_tiny(D, nat);
     if (mapped) {
         dv = c->se_hdev;
@@ -972,6 +972,12 @@ int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, doubl
     a.energy = (double*)(dv + SmallEvalIo::energy);
     a.acc = (int*)(dv + SmallEvalIo::acc);
     a.eval_only = 1;
+    if (mapped) {
+        // the item-parallel form takes the positions and element indices with
+        // the launch and writes its results into the mapped block
+        a.inline_pos = (const double*)(h + SmallEvalIo::pos);
+        a.inline_elem = he;
+    }
     launch_small_md(b, D, a, st);
     CUDA_TRY(cudaGetLastError());
     const size_t out = SmallEvalIo::force + sizeof(double) * 3 * nat - SmallEvalIo::out_off;

@@ -273,6 +273,11 @@ struct SmallMdArgs {
     double* hist;       // [nsteps] energies or null
     int* acc;           // [2]: OR of status flags, evaluations
     int eval_only;      // 1: one evaluation of pos (nsteps 1), no MD; mom and mass unused
+    // host copies of the positions and element indices of an evaluation,
+    // passed with the launch of the item-parallel form (null: read pos and
+    // the batch's element indices from memory)
+    const double* inline_pos = nullptr;
+    const int* inline_elem = nullptr;
 };
 
 // packed image shift: three signed 8-bit lattice multiples

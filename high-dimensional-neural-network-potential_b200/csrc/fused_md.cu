@@ -22,6 +22,8 @@
 // Neighbours are listed in atom-index order (the reference walks its cell
 // grid; for a molecule both give the same set, the sums differ only in
 // rounding).
+#include <atomic>
+
 #include "engine.h"
 #include "mlp_tile.cuh"
 #include "symfn_generic.cuh"
@@ -374,6 +376,12 @@ struct TinyArgs {
     int* acc;
     const int* elem;
     int eval_only;                  // 1: one evaluation of pos, no MD (mom, mass unused)
+    // 1: positions and element indices are the copies below, passed with the
+    // launch (the plain call of one molecule: no copy and no read of host
+    // memory from the kernel)
+    int inline_in;
+    double in_pos[3 * kSmallMolecule];
+    int in_elem[kSmallMolecule];
 };
 
 // pair r of one centre's list (0 <= p < q): r = q (q - 1) / 2 + p
@@ -433,13 +441,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
     int* blkof = (int*)(smem + a.slot[tBlkOf]);      // block of an element pair
     int* status = (int*)(smem + a.slot[tStatus]);
     for (int q = tid; q < n3; q += nt) {
-        pos[q] = a.pos[q];
+        pos[q] = a.inline_in ? a.in_pos[q] : a.pos[q];
         mom[q] = a.eval_only ? 0.0 : a.mom[q];
         F[q] = a.eval_only ? 0.0 : a.force[q];
     }
     for (int i = tid; i < N; i += nt) {
         mass[i] = a.eval_only ? 1.0 : a.mass[i];
-        elem[i] = a.elem[i];
+        elem[i] = a.inline_in ? a.in_elem[i] : a.elem[i];
     }
     for (int x = tid; x < nel * nblk; x += nt)
         for (int g = m.g4_off[x]; g < m.g4_off[x + 1]; ++g) recblk[g] = x % nblk;
@@ -790,8 +798,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
         a.force[q] = F[q];
     }
     if (tid == 0) {
-        a.acc[0] |= status[0];
-        a.acc[1] += a.nsteps;
+        if (a.eval_only) {
+            // the caller cleared acc; plain stores (acc may be mapped host
+            // memory, where a read-modify-write costs a bus round trip)
+            a.acc[0] = status[0];
+            a.acc[1] = a.nsteps;
+        } else {
+            a.acc[0] |= status[0];
+            a.acc[1] += a.nsteps;
+        }
     }
 }
 
@@ -855,7 +870,27 @@ int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& x, cud
         ta.acc = x.acc;
         ta.elem = b.elem;
         ta.eval_only = x.eval_only;
-        cudaFuncSetAttribute(k_tiny_md, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+        if (x.inline_pos && x.inline_elem && x.natoms <= kSmallMolecule) {
+            ta.inline_in = 1;
+            for (int q = 0; q < 3 * x.natoms; ++q) ta.in_pos[q] = x.inline_pos[q];
+            for (int i = 0; i < x.natoms; ++i) ta.in_elem[i] = x.inline_elem[i];
+        }
+        // the shared-memory limit is raised once per device and size (the
+        // attribute call costs about a microsecond)
+        {
+            constexpr int kMaxDev = 64;
+            static std::atomic<size_t> raised[kMaxDev];
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev < 0 || dev >= kMaxDev || raised[dev].load(std::memory_order_relaxed) < tsm) {
+                cudaFuncSetAttribute(k_tiny_md, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+                if (dev >= 0 && dev < kMaxDev) {
+                    size_t cur = raised[dev].load(std::memory_order_relaxed);
+                    while (cur < tsm && !raised[dev].compare_exchange_weak(cur, tsm)) {
+                    }
+                }
+            }
+        }
         k_tiny_md<<<1, kThreads, tsm, s>>>(m, ta);
         return 1;
     }
