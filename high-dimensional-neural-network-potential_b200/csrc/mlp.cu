@@ -98,7 +98,7 @@ __host__ __device__ inline int dmma_stride(int maxw) { return (maxw + 1) | 1; }
 // the forward pass, deltas in the backward pass), [8][stride] each
 __host__ __device__ inline int dmma_warp_doubles(int L, int stride) { return (L + 2) * kDR * stride; }
 
-__global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int S) {
+__global__ void __launch_bounds__(32 * kDW, 6) k_mlp_dmma(Batch b, DevModel m, int S) {
     extern __shared__ __align__(16) double dsm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int L = m.nlayers;
@@ -130,25 +130,40 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
     const double* grow = atom >= 0 ? b.G + (size_t)atom * nsf : nullptr;
     const double* F = m.dm_fwd + m.dm_off_f[e] + lane;  // [ks][nt][32]
     const int KS = (nin + 3) >> 2;
-    double a_n = (grow && q < nin) ? __ldg(grow + q) : 0.0;
-    double b_n[4];
+    // operands of k-step ks (zero A and no B load beyond the last step)
+    auto load = [&](int ks, double& a, double (&bf)[4]) {
+        const int k = 4 * ks + q;
+        a = (grow && k < nin) ? __ldg(grow + k) : 0.0;
+        if (ks < KS) {
+            const double* f = F + (size_t)ks * 128;
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt) b_n[nt] = __ldg(F + nt * 32);
-#pragma unroll 2
-    for (int ks = 0; ks < KS; ++ks) {
-        const double a = a_n;
-        double bb[4];
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) bb[nt] = b_n[nt];
-        if (ks + 1 < KS) {
-            const int k = 4 * (ks + 1) + q;
-            a_n = (grow && k < nin) ? __ldg(grow + k) : 0.0;
-            const double* f = F + (size_t)(ks + 1) * 128;
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) b_n[nt] = __ldg(f + nt * 32);
+            for (int nt = 0; nt < 4; ++nt) bf[nt] = __ldg(f + nt * 32);
         }
+    };
+    // two k-steps in flight: the operands of ks + 2 are loaded while ks
+    // multiplies (two register sets, the loop unrolled by two)
+    double a0 = 0.0, a1 = 0.0, b0[4] = {0.0, 0.0, 0.0, 0.0}, b1[4] = {0.0, 0.0, 0.0, 0.0};
+    load(0, a0, b0);
+    load(1, a1, b1);
+    for (int ks = 0; ks < KS; ks += 2) {
+        {
+            const double a = a0;
+            double bb[4];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) dmma(acc[nt], a, bb[nt]);
+            for (int nt = 0; nt < 4; ++nt) bb[nt] = b0[nt];
+            if (ks + 2 < KS) load(ks + 2, a0, b0);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) dmma(acc[nt], a, bb[nt]);
+        }
+        if (ks + 1 < KS) {
+            const double a = a1;
+            double bb[4];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) bb[nt] = b1[nt];
+            if (ks + 3 < KS) load(ks + 3, a1, b1);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) dmma(acc[nt], a, bb[nt]);
+        }
     }
     {
         const double* b1 = m.b + m.b_off[e * L];
@@ -169,7 +184,9 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
     // hidden and output layers: lane = output neuron, the warp's 8 atoms
     for (int l = 1; l < L; ++l) {
         const int win = m.width[l], wout = m.width[l + 1];
-        const double* W = m.w + m.w_off[e * L + l];  // [wout][win]
+        // transposed weights [win][wout]: the lanes' loads of one input are
+        // one coalesced row
+        const double* WT = m.wt + m.w_off[e * L + l];
         const double* bl = m.b + m.b_off[e * L + l];
         const double* yin = yb((l - 1) & 1);
         double* yout = yb(l & 1);
@@ -178,7 +195,7 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
 #pragma unroll
             for (int rr = 0; rr < kDR; ++rr) sacc[rr] = 0.0;
             for (int i = 0; i < win; ++i) {
-                const double w = W[(size_t)lane * win + i];
+                const double w = __ldg(WT + (size_t)i * wout + lane);
 #pragma unroll
                 for (int rr = 0; rr < kDR; ++rr) sacc[rr] += w * yin[rr * S + i];
             }
@@ -207,13 +224,19 @@ __global__ void __launch_bounds__(32 * kDW) k_mlp_dmma(Batch b, DevModel m, int 
     for (int l = L - 1; l >= 1; --l) {
         const int wout = m.width[l + 1], wi = m.width[l];
         const double* W = m.w + m.w_off[e * L + l];  // [wout][wi]
-        if (lane < wi)
+        if (lane < wi) {
+            // each weight loaded once for the warp's 8 atoms (same sum order)
+            double sv[kDR];
 #pragma unroll
-            for (int rr = 0; rr < kDR; ++rr) {
-                double sv = 0.0;
-                for (int o = 0; o < wout; ++o) sv += dcur[rr * S + o] * W[(size_t)o * wi + lane];
-                dnext[rr * S + lane] = sv * da(l - 1)[rr * S + lane];
+            for (int rr = 0; rr < kDR; ++rr) sv[rr] = 0.0;
+            for (int o = 0; o < wout; ++o) {
+                const double w = __ldg(W + (size_t)o * wi + lane);
+#pragma unroll
+                for (int rr = 0; rr < kDR; ++rr) sv[rr] += dcur[rr * S + o] * w;
             }
+#pragma unroll
+            for (int rr = 0; rr < kDR; ++rr) dnext[rr * S + lane] = sv[rr] * da(l - 1)[rr * S + lane];
+        }
         __syncwarp();
         double* t = dcur;
         dcur = dnext;
