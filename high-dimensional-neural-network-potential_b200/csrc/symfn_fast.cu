@@ -598,13 +598,18 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         // blocks, and a block's remainder is carried into the next block's
         // chunks instead of being flushed as a partly filled chunk.
         // FP32 with two lambdas: the accumulators packed over lambda,
-        // acc2[z * NE + e] = (acc[0, z, e], acc[1, z, e]).
+        // acc2[z * NE + e] = (acc[0, z, e], acc[1, z, e]).  FP64 with two
+        // lambdas: the lambdas split over a lane pair (lane, lane ^ 1), each
+        // lane adding lambda_(lane & 1) of both pairs' terms, acc[z * NE + e]
+        // (half the accumulators and half the reduction per lane).
         constexpr bool kPk = sizeof(T) == 4 && NL == 2;
-        T acc[P];
+        constexpr bool kSp = sizeof(T) == 8 && NL == 2;
+        constexpr int NA = kSp ? P / 2 : P;
+        T acc[NA];
         float2 acc2[kPk ? NZ * NE : 1];
         auto zero_acc = [&]() {
 #pragma unroll
-            for (int p = 0; p < P; ++p) acc[p] = (T)0;
+            for (int p = 0; p < NA; ++p) acc[p] = (T)0;
 #pragma unroll
             for (int p = 0; p < (kPk ? NZ * NE : 1); ++p) acc2[p] = f2(0.0f);
         };
@@ -636,6 +641,14 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 for (int z = 0; z < NZ; ++z)
 #pragma unroll
                     for (int e = 0; e < NE; ++e) acc2[z * NE + e] = __ffma2_rn(Tz[z], f2((float)Y[e]), acc2[z * NE + e]);
+            } else if constexpr (kSp) {
+                const T lam = (lane & 1) ? (T)m.lam[1] : (T)m.lam[0];
+                T Tz[NZ], Tp[NZ];
+                powers<S, false>(m, (T)1 + lam * cth, Tz, Tp);
+#pragma unroll
+                for (int z = 0; z < NZ; ++z)
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) acc[z * NE + e] += Tz[z] * Y[e];
             } else {
 #pragma unroll
                 for (int l = 0; l < NL; ++l) {
@@ -651,6 +664,33 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         // every lane's sums of block t -> G of block t (warp reduction through
         // shared memory, row stride P+1); called by all lanes
         auto emit = [&](int t) {
+            if constexpr (kSp) {
+                // rows of P/2: lane L holds lambda_(L & 1); output p = (l, z, e)
+                // sums the 16 rows of parity l, 32/P helper lanes per output
+                T* row = s.red + lane * (P / 2 + 1);
+#pragma unroll
+                for (int q = 0; q < P / 2; ++q) row[q] = acc[q];
+                __syncwarp();
+                constexpr int NH = 32 / P > 0 ? 32 / P : 1;
+                static_assert(16 % NH == 0, "helpers per output");
+                const int p = lane % P, hh = lane / P;
+                const int l = p / (NZ * NE), q = p % (NZ * NE);
+                T sum = (T)0;
+                if (hh < NH)
+#pragma unroll
+                    for (int r = 0; r < 16 / NH; ++r) sum += s.red[(2 * (hh + r * NH) + l) * (P / 2 + 1) + q];
+#pragma unroll
+                for (int off = P; off < 32; off <<= 1) sum += __shfl_xor_sync(kFull, sum, off);
+                __syncwarp();
+                if (lane < P) {
+                    const int sf = m.pmap[((size_t)c * m.nblk + t) * P + lane];
+                    if (sf >= 0) {
+                        const int z = (lane / NE) % NZ;
+                        Gi[sf] = (T)(((double)((T)m.pfz[z] * sum) - mean[sf]) * iwidth[sf]);
+                    }
+                }
+                return;
+            }
             {
                 T* row = s.red + lane * (P + 1);
                 if constexpr (kPk) {
@@ -702,13 +742,32 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
                 // FP64: one call site of the accumulation, in two passes
                 // around the reduction (smaller code: the value pass was
                 // instruction-fetch bound; 24.7 against 25.4 ms on the C4 batch)
+                // with the lambda split this lane also takes its partner's
+                // (lane ^ 1) pair: its terms come by shuffle
+                T cth_o = (T)0, Y_o[NE];
+                int tg_o = cur;
+                const bool live_o = kSp && (lane ^ 1) < n;
+                if constexpr (kSp) {
+                    cth_o = __shfl_xor_sync(kFull, cth, 1);
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) Y_o[e] = __shfl_xor_sync(kFull, Y[e], 1);
+                    tg_o = __shfl_xor_sync(kFull, tg, 1);
+                }
                 for (int pass = 0; pass < (straddle ? 2 : 1); ++pass) {
                     if (pass == 1) {
                         emit(cur);
                         zero_acc();
                         cur = nxt;
                     }
-                    if (lane < n && tg == cur) accumulate(cth, Y);
+                    for (int w2 = 0; w2 < (kSp ? 2 : 1); ++w2) {
+                        const bool own = w2 == 0;
+                        if (own ? (lane < n && tg == cur) : (live_o && tg_o == cur)) {
+                            T Yw[NE];
+#pragma unroll
+                            for (int e = 0; e < NE; ++e) Yw[e] = own ? Y[e] : Y_o[e];
+                            accumulate(own ? cth : cth_o, Yw);
+                        }
+                    }
                 }
             } else if (!straddle) {
                 // FP32 at 72 registers: the two-pass loop spills (70.4 against 73.0 ms)
