@@ -194,6 +194,9 @@ __global__ void __launch_bounds__(32 * kDW, 6) k_mlp_dmma(Batch b, DevModel m, i
             double sacc[kDR];
 #pragma unroll
             for (int rr = 0; rr < kDR; ++rr) sacc[rr] = 0.0;
+            // unrolled so that several weight loads are in flight (they come
+            // from L2: the shared memory of 6 blocks leaves no L1)
+#pragma unroll 5
             for (int i = 0; i < win; ++i) {
                 const double w = __ldg(WT + (size_t)i * wout + lane);
 #pragma unroll
@@ -229,6 +232,7 @@ __global__ void __launch_bounds__(32 * kDW, 6) k_mlp_dmma(Batch b, DevModel m, i
             double sv[kDR];
 #pragma unroll
             for (int rr = 0; rr < kDR; ++rr) sv[rr] = 0.0;
+#pragma unroll 5
             for (int o = 0; o < wout; ++o) {
                 const double w = __ldg(W + (size_t)o * wi + lane);
 #pragma unroll
