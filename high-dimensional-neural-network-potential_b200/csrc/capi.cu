@@ -12,6 +12,7 @@
 
 #include "../../include/hdnnp_gpu.h"
 #include "engine.h"
+#include "fastmath.cuh"
 #include "model.h"
 
 using namespace hdnnp;
@@ -1569,6 +1570,44 @@ int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches) {
 }
 
 }  // extern "C"
+
+// ====================================================================== math check
+// hdnnp_debug_math: the branch-free FP64 functions of fastmath.cuh (used by
+// the symmetry-function kernels) evaluated on the device over a host array,
+// so that tests can hold them against the library functions.
+namespace {
+__global__ void k_math_check(int which, int n, const double* x, double* y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = x[i];
+    double r = 0.0, ir = 0.0;
+    switch (which) {
+        case 0: r = exp_clamped(v); break;
+        case 1: r = tanh01(v); break;
+        case 2: sqrt_rsqrt(v, r, ir); break;
+        default: r = rsqrt_pos(v); break;
+    }
+    y[i] = r;
+}
+}  // namespace
+
+extern "C" int hdnnp_debug_math(int which, int n, const double* x, double* y) {
+    if (which < 0 || which > 3) return fail(HDNNP_E_INPUT, "which must be 0 (exp), 1 (tanh), 2 (sqrt) or 3 (1/sqrt)");
+    if (n < 0 || (n > 0 && (!x || !y))) return fail(HDNNP_E_INPUT, "null argument or negative count");
+    if (n == 0) return HDNNP_OK;
+    double* d = nullptr;
+    const size_t bytes = sizeof(double) * (size_t)n;
+    CUDA_TRY(cudaMalloc(&d, 2 * bytes));
+    cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_math_check<<<(n + 255) / 256, 256>>>(which, n, d, d + n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(HDNNP_E_CUDA, std::string("hdnnp_debug_math: ") + cudaGetErrorString(e));
+    return HDNNP_OK;
+}
 
 // ====================================================================== no-allocation entry point
 // hdnnp_energy_and_forces_noalloc: the evaluation of hdnnp_energy_and_forces

@@ -17,8 +17,9 @@
 //    Estrin's scheme (depth 4 instead of a 13-deep Horner chain), 1 added
 //    last; 2^k applied through the exponent field (e^-708 ~ 3e-308, the
 //    smallest result without a subnormal scale).  Error within 1 ulp of
-//    the correctly rounded result (the same operations emulated on the
-//    host with exact fused multiply-adds, against libm, 2e4 arguments).
+//    libm (tests/test_fastmath.py emulates these operations on the host
+//    with exact fused multiply-adds, and checks the device functions, run
+//    through hdnnp_debug_math, against libm's exp, tanh and sqrt).
 //  * tanh01(u) = (1 - e^(-2u)) / (1 + e^(-2u)) with the quotient from the
 //    hardware reciprocal approximation refined by one third-order Newton
 //    step and one residual correction (Newton-Raphson division, as in

@@ -82,6 +82,7 @@ def lib():
     L.hdnnp_dEdLat_to_stress.argtypes = [D, D, D]
     L.hdnnp_debug_fetch.argtypes = [P, C.c_char_p, P, C.c_size_t]
     L.hdnnp_last_launch_count.argtypes = [P, C.POINTER(C.c_int)]
+    L.hdnnp_debug_math.argtypes = [C.c_int, C.c_int, D, D]
     L.hdnnp_ctx_set_profiling.argtypes = [P, C.c_int]
     L.hdnnp_profile_read.argtypes = [P, D, I64, C.c_int]
     L.hdnnp_committee_energy_and_forces.argtypes = [P, P, C.c_int, C.c_int, I, D, C.c_int, D, D, D, D, D]
@@ -374,6 +375,15 @@ def dEdLat_to_stress(lat, dEdLat):
     dl = np.asarray(dEdLat, dtype=np.float64).ravel(order="F").copy()
     _check(lib().hdnnp_dEdLat_to_stress(_dp(L), _dp(dl), _dp(out)))
     return out.reshape(3, 3, order="F")
+
+
+def debug_math(which: int, x) -> np.ndarray:
+    """The branch-free FP64 exp (0), tanh on [0, 1] (1), sqrt (2) and 1/sqrt
+    (3) of the symmetry-function kernels, evaluated on the current device."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    _check(lib().hdnnp_debug_math(which, x.size, _dp(x), _dp(y)))
+    return y
 
 
 def exported_symbols(header: str):

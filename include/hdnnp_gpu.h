@@ -257,6 +257,14 @@ int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes);
 /* Kernel launches issued by the last evaluation on `c`. */
 int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches);
 
+/* The branch-free FP64 functions that the symmetry-function kernels use for
+ * their bounded arguments, evaluated on the current device: y[i] = f(x[i]),
+ * which = 0 exp (arguments clamped to [-708, 709]), 1 tanh (u in [0, 1]),
+ * 2 sqrt, 3 1/sqrt.  No reference counterpart (a test hook; the reference
+ * calls the Fortran intrinsics exp, tanh and sqrt in
+ * symmetryFunctions.f90:201-327).                                            */
+int hdnnp_debug_math(int which, int n, const double* x, double* y);
+
 /* ---------------------------------------------------------------- profiling
  * Tracing hook in place of the reference's per-stage cpu_time prints
  * (hdnnps.f90:346-368), which are always on there.  With profiling enabled
