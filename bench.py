@@ -84,6 +84,25 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, world, device):
+    """The largest of the ranks' values of x: a job of replicas is as fast as
+    its slowest rank.  With one rank, x itself."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_value(atoms_per_rank, world, steps, seconds):
+    """Whole-job atom-steps/s of `world` replicas that each evaluate their own
+    batch of `atoms_per_rank` atoms `steps` times in `seconds` (the slowest
+    rank's time)."""
+    return atoms_per_rank * world * steps / seconds
+
+
 def workload(W, n, seed):
     structs = W.config_c4(n_struct=n, seed=seed)
     off, Z, pos, lat, per = W.concat(structs)
@@ -688,11 +707,8 @@ def main():
     stage_ms, counters = bplan.profile(reset=True)
     dev_s = sum(a.elapsed_time(b) for a, b in times) / 1e3
     launches_per_step = bplan.info()["kernels_per_launch"]
-    t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_s = float(t.item())
-    value = natoms * world * args.steps / dev_s
+    dev_s = max_over_ranks(dev_s, world, "cuda")
+    value = weak_value(natoms, world, args.steps, dev_s)
     if args.lean:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "ms_per_step": dev_s / args.steps * 1e3,
@@ -741,18 +757,15 @@ def main():
         for _ in range(n):
             fn()  # returns after this step's D2H copies completed
         barrier()
-        t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(time.perf_counter() - t0, world, "cuda")
 
     for _ in range(max(1, args.warmup // 2)):
         step_host_plan()
         step_host()
-    e2e = natoms * world * args.steps / wall(step_host_plan, args.steps)
+    e2e = weak_value(natoms, world, args.steps, wall(step_host_plan, args.steps))
     bplan.sync(stream.cuda_stream)  # device flags of the e2e steps (raises on an error)
     bplan.profile(reset=True)
-    e2e_eager = natoms * world * args.steps / wall(step_host, args.steps)
+    e2e_eager = weak_value(natoms, world, args.steps, wall(step_host, args.steps))
     h2d = Z.nbytes + pos.nbytes
     d2h = (Eh.numel() + Fh.numel() + Lh.numel()) * 8
 

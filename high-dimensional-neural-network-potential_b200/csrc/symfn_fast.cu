@@ -1107,9 +1107,13 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 8 : 5) k_sfg_fas
         const int np = b.pairs ? b.npairs[i] : -1;
         if (np >= 0 && np <= b.pcap) {
             const unsigned* pl = b.pairs + (size_t)i * b.pcap;
+            // the next chunk's entries are loaded while this chunk computes
+            unsigned nxt = lane < np ? __ldg(pl + lane) : 0u;
             for (int base = 0; base < np; base += 32) {
                 const int n = np - base < 32 ? np - base : 32;
-                grad_pairs<T, S>(s, m, ne, rc, inv_rc, rc2d, lane < n ? pl[base + lane] : 0u, n, lane);
+                const unsigned pk = nxt;
+                if (base + 32 < np) nxt = base + 32 + lane < np ? __ldg(pl + base + 32 + lane) : 0u;
+                grad_pairs<T, S>(s, m, ne, rc, inv_rc, rc2d, lane < n ? pk : 0u, n, lane);
                 __syncwarp();
             }
         } else {
