@@ -662,7 +662,8 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             }
         };
         // every lane's sums of block t -> G of block t (warp reduction through
-        // shared memory, row stride P+1); called by all lanes
+        // shared memory: rows of P + 1, or of P/2 + 1 with the lambda split);
+        // called by all lanes
         auto emit = [&](int t) {
             if constexpr (kSp) {
                 // rows of P/2: lane L holds lambda_(L & 1); output p = (l, z, e)
@@ -741,9 +742,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
             if constexpr (sizeof(T) == 8) {
                 // FP64: one call site of the accumulation, in two passes
                 // around the reduction (smaller code: the value pass was
-                // instruction-fetch bound; 24.7 against 25.4 ms on the C4 batch)
-                // with the lambda split this lane also takes its partner's
-                // (lane ^ 1) pair: its terms come by shuffle
+                // instruction-fetch bound; 24.7 against 25.4 ms on the C4
+                // batch).  With the lambda split this lane also takes its
+                // partner's (lane ^ 1) pair, whose terms come by shuffle.
                 T cth_o = (T)0, Y_o[NE];
                 int tg_o = cur;
                 const bool live_o = kSp && (lane ^ 1) < n;
