@@ -815,7 +815,7 @@ def main():
         compare["plain_sample"] = f"{len(sample)} structures ({atoms} atoms), hdnnp_energy_and_forces with host arrays"
         mixed_v = value if args.precision == "mixed" else compare["batched_mixed"]
         fp64_v = value if args.precision == "fp64" else compare["batched_fp64"]
-        compare["north_star"] = {
+        compare["speedup_ratios"] = {
             "target": "batched/served mixed >= 5x the plain FP64 GPU path on the same mixed-size workload",
             "mixed_over_plain_fp64_per_structure": mixed_v / compare["plain_fp64_per_structure"],
             "mixed_over_batched_fp64": mixed_v / fp64_v,
@@ -825,7 +825,7 @@ def main():
             pot.set_precision(engine.HDNNP_PREC_MIXED)
             compare["served"] = serve_leg(pkg, engine, pot, engine.HDNNP_PREC_MIXED, args.serve_seconds)
             compare["served"]["precision"] = "mixed"
-            compare["north_star"]["served_mixed_over_plain_fp64_per_structure"] = (
+            compare["speedup_ratios"]["served_mixed_over_plain_fp64_per_structure"] = (
                 compare["served"]["saturation"]["atom_steps_per_s"] / compare["plain_fp64_per_structure"])
             pot.set_precision(prec)
         if world == 1 and args.md:
