@@ -579,7 +579,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(T) == 4 ? 7 : 4) k_sfv_fas
         // slower in both precisions: 25.4 against 20.8 ms per C4 step in
         // FP64, 14.9 against 12.8 in FP32.  Groups of lanes per neighbour
         // element, each lane a function and a share of the neighbours, with a
-        // butterfly over the groups, were slower too: 21.4 against 20.5.)
+        // butterfly over the groups, gained nothing.)
         const int r0 = m.g2_off[c * nel], r1 = m.g2_off[c * nel + nel];
         for (int f = r0 + lane; f < r1; f += 32) {
             const SF2 q = m.g2[f];
