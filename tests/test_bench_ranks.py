@@ -1,9 +1,9 @@
-"""bench.py with several ranks (replicas, one process per GPU) on CPU: two
+"""bench.py host logic on CPU.  Several ranks (replicas, one process per GPU) as two
 gloo ranks on 127.0.0.1.  The path has no data-path collective; the ranks
 meet only for the slowest rank's time (max over ranks) and a barrier.
 Checked here: the max over ranks, the weak-scaling value, per-rank batches
-(seed 4 + rank: different structures of the same kind) and that the
-reference arm runs on rank 0 alone."""
+(seed 4 + rank: different structures of the same kind), that the
+reference arm runs on rank 0 alone, and the reference arm's JSON line."""
 import io
 import os
 import socket
@@ -76,3 +76,23 @@ def test_reference_arm_runs_on_rank_zero_only():
     with redirect_stdout(buf):
         assert bench.run_reference(args, 1, 2) is None
     assert buf.getvalue() == ""
+
+
+def test_reference_arm_line_on_cpu():
+    """bench.py --impl reference: the reference's algorithm (the oracle source
+    built -O3 -march=native -fopenmp on this host) on the host cores prints one
+    JSON line with the contract's keys; no GPU involved."""
+    import json
+    import subprocess
+
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--structs", "16",
+                        "--steps", "1", "--warmup", "0", "--cpu-sample", "32"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "atom-steps/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["dtype"] == "f64"
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
