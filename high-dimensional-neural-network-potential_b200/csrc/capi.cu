@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -209,6 +211,16 @@ struct hdnnp_ctx {
     // "small_eval", default on).  se_dev: the io block (see small_eval_io)
     // and the kernel's global homes; se_host: its mapped pinned mirror.
     int small_eval = 1;
+    // the resident form of that kernel (option "small_resident", default on):
+    // a single-block kernel that stays on one SM between calls and serves
+    // them from a mapped-memory mailbox (no launch per call, warm caches); it
+    // exits by itself after a few idle milliseconds
+    int small_resident = 1;
+    ResidentBox* rs_box = nullptr;     // mailbox, mapped pinned host memory
+    ResidentBox* rs_dbox = nullptr;    // its device address
+    cudaStream_t rs_stream = nullptr;  // non-blocking stream of the resident kernel
+    int rs_natoms = 0;                 // atoms the running kernel serves (0: none launched)
+    int rs_seq = 0;                    // number of the last request
     void* se_dev = nullptr;
     unsigned char* se_host = nullptr;
     unsigned char* se_hdev = nullptr;  // device address of the mapped se_host
@@ -226,6 +238,12 @@ struct hdnnp_ctx {
     bool have_last = false;
     std::vector<StructInfo> hinfo;
     ~hdnnp_ctx() {
+        if (rs_natoms && rs_box) {  // stop the resident kernel first (a cudaFree would wait for it)
+            rs_box->quit = 1;
+            std::atomic_thread_fence(std::memory_order_seq_cst);
+            cudaStreamSynchronize(rs_stream);
+            rs_natoms = 0;
+        }
         for (auto* b : {&Z, &sid, &elem, &cell_of, &cell_cnt, &cell_start, &cell_atoms, &nei_cnt, &nei_off, &nei_j,
                         &nei_s, &nei_rev, &el_count, &el_start, &el_atoms, &scan_tmp, &status})
             b->release();
@@ -243,6 +261,8 @@ struct hdnnp_ctx {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (h_status) cudaFreeHost(h_status);
+        if (rs_box) cudaFreeHost((void*)rs_box);
+        if (rs_stream) cudaStreamDestroy(rs_stream);
         if (se_dev) cudaFree(se_dev);
         if (se_host) cudaFreeHost(se_host);
         if (stream) cudaStreamDestroy(stream);
@@ -933,14 +953,86 @@ int small_eval_setup(hdnnp_ctx* c) {
     return HDNNP_OK;
 }
 
+// Stops the context's resident kernel (if one runs) and waits for it.
+int resident_stop(hdnnp_ctx* c) {
+    if (!c->rs_natoms) return HDNNP_OK;
+    c->rs_box->quit = 1;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    CUDA_TRY(cudaStreamSynchronize(c->rs_stream));
+    c->rs_natoms = 0;
+    return HDNNP_OK;
+}
+
+// One molecule through the resident item-parallel kernel: the inputs and a
+// request number go into the mailbox, the kernel (launched on the first
+// call, or again when the molecule's size changes or the kernel left after
+// idling) answers with the outputs and the number.  Every field of the
+// mailbox has one writer, so a kernel that left just before the request
+// came is seen (exited) and replaced, and the new kernel serves the pending
+// request.  The host waits at most 2 s.
+int small_eval_resident(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, double* energy, double* force) {
+    const DevModel& D = c->model->dev;
+    if (!c->rs_box) {
+        CUDA_TRY(cudaHostAlloc((void**)&c->rs_box, sizeof(ResidentBox), cudaHostAllocMapped));
+        std::memset((void*)c->rs_box, 0, sizeof(ResidentBox));
+        CUDA_TRY(cudaHostGetDevicePointer((void**)&c->rs_dbox, (void*)c->rs_box, 0));
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->rs_stream, cudaStreamNonBlocking));
+    }
+    ResidentBox* bx = c->rs_box;
+    int r;
+    if (c->rs_natoms && c->rs_natoms != nat && (r = resident_stop(c))) return r;
+    bx->natoms = nat;
+    std::memcpy(bx->pos, pos, sizeof(double) * 3 * nat);
+    for (int i = 0; i < nat; ++i) bx->elem[i] = D.z2e[Z[i]];
+    bx->acc[0] = bx->acc[1] = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    const int seq = ++c->rs_seq;
+    bx->req = seq;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    c->launches = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        if (!c->rs_natoms) {
+            bx->quit = 0;
+            bx->exited = 0;
+            std::atomic_thread_fence(std::memory_order_seq_cst);
+            if (!launch_small_resident(D, nat, c->rs_dbox, c->rs_stream))
+                return fail(HDNNP_E_STATE, "molecule does not take the resident single-block form");
+            CUDA_TRY(cudaGetLastError());
+            c->rs_natoms = nat;
+            c->launches = 1;
+        }
+        if (bx->ack == seq) break;
+        if (bx->exited) {  // it left, idle, before it saw this request: replace it
+            CUDA_TRY(cudaStreamSynchronize(c->rs_stream));
+            c->rs_natoms = 0;
+            continue;
+        }
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(2)) {
+            resident_stop(c);
+            return fail(HDNNP_E_STATE, "the resident single-block kernel did not answer within 2 s");
+        }
+    }
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    c->have_last = false;
+    const int st = bx->acc[0];
+    if (st & 8) return fail(HDNNP_E_INPUT, "non-finite position (structure 0)");
+    if (st) return fail(HDNNP_E_STATE, "single-block evaluation: device flags " + std::to_string(st));
+    *energy = bx->energy;
+    std::memcpy(force, bx->force, sizeof(double) * 3 * nat);
+    return HDNNP_OK;
+}
+
 // One molecule of nat <= kSmallMolecule atoms in FP64 through the
 // single-block kernel (fused_md.cu, evaluation mode): one kernel and one
 // wait (plus a host-to-device and a device-to-host copy when the
-// warp-per-atom form runs).  Z must be validated.
+// warp-per-atom form runs), or a request to the context's resident kernel
+// (item-parallel form, option small_resident).  Z must be validated.
 int small_eval(hdnnp_ctx* c, int nat, const int32_t* Z, const double* pos, double* energy, double* force) {
     int r;
-    if ((r = small_eval_setup(c))) return r;
     const DevModel& D = c->model->dev;
+    if (c->small_resident && small_md_tiny(D, nat)) return small_eval_resident(c, nat, Z, pos, energy, force);
+    if ((r = small_eval_setup(c))) return r;
     unsigned char* h = c->se_host;
     unsigned char* dv = (unsigned char*)c->se_dev;
     std::memcpy(h + SmallEvalIo::pos, pos, sizeof(double) * 3 * nat);
@@ -1174,6 +1266,10 @@ int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value) {
         if (value < 0 || value > 64) return fail(HDNNP_E_INPUT, "sf_blocks_per_sm must be 0..64");
         c->sf_blocks_per_sm = value;
         return HDNNP_OK;
+    }
+    if (std::string(name) == "small_resident") {
+        c->small_resident = value != 0;
+        return c->small_resident ? HDNNP_OK : resident_stop(c);
     }
     if (std::string(name) == "small_eval") {
         c->small_eval = value != 0;

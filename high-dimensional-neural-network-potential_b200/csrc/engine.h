@@ -324,11 +324,39 @@ size_t mlp_tc_smem_bytes(const DevModel& m);
 
 size_t sf_smem_per_warp(int mmax, bool grad);
 int device_sm_count();  // multiprocessors of the current device (cached per device)
+// Mailbox of the resident single-block kernel (mapped pinned host memory,
+// one per context): the host writes a request's inputs and then `req`; the
+// kernel serves it, writes the outputs and then `ack`.  Every field has one
+// writer (host: req, quit, natoms, pos, elem; kernel: ack, exited, acc,
+// energy, force).
+struct ResidentBox {
+    volatile int req;      // sequence number of the newest request
+    volatile int ack;      // sequence number of the last request served
+    volatile int quit;     // 1: leave the loop now
+    volatile int exited;   // 1: the kernel has left its loop
+    int natoms;
+    int acc[2];            // status flags of the last request, evaluations (1)
+    int pad;
+    double energy;
+    double pos[3 * kSmallMolecule];
+    int elem[kSmallMolecule];
+    double force[3 * kSmallMolecule];
+};
+// Polls of an idle resident kernel before it exits (each poll a read of
+// host memory, about a microsecond: a few milliseconds).
+constexpr int kResidentPolls = 4000;
+
 size_t small_md_smem_bytes(const DevModel& m, int natoms);  // dynamic shared memory of the kernel
 // true when the item-parallel form runs: it reads its inputs once into
 // shared memory and writes its outputs once (host-mapped buffers are fine)
 bool small_md_tiny(const DevModel& m, int natoms);
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& a, cudaStream_t s);
+// The item-parallel single-block kernel in resident mode for molecules of
+// `natoms` atoms: it serves evaluation requests from the mailbox `box` (its
+// device address) until `quit` or until it has polled kResidentPolls times
+// without a request.  Returns 0 if the molecule does not take the
+// item-parallel form.
+int launch_small_resident(const DevModel& m, int natoms, ResidentBox* box, cudaStream_t s);
 
 // Compiled product-space shapes of the fast SF kernels: id -> (NL, NZ, NE).
 // Ids 1-4 read zeta from the model; ids 5-6 have the zeta set compiled in

@@ -382,6 +382,9 @@ struct TinyArgs {
     int inline_in;
     double in_pos[3 * kSmallMolecule];
     int in_elem[kSmallMolecule];
+    // resident mode: serve evaluation requests from this mailbox (device
+    // address of mapped host memory) until told to quit or idle
+    ResidentBox* box;
 };
 
 // pair r of one centre's list (0 <= p < q): r = q (q - 1) / 2 + p
@@ -440,20 +443,52 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
     int* recblk = (int*)(smem + a.slot[tRecBlk]);    // block of each angular record
     int* blkof = (int*)(smem + a.slot[tBlkOf]);      // block of an element pair
     int* status = (int*)(smem + a.slot[tStatus]);
-    for (int q = tid; q < n3; q += nt) {
-        pos[q] = a.inline_in ? a.in_pos[q] : a.pos[q];
-        mom[q] = a.eval_only ? 0.0 : a.mom[q];
-        F[q] = a.eval_only ? 0.0 : a.force[q];
-    }
-    for (int i = tid; i < N; i += nt) {
-        mass[i] = a.eval_only ? 1.0 : a.mass[i];
-        elem[i] = a.inline_in ? a.in_elem[i] : a.elem[i];
-    }
     for (int x = tid; x < nel * nblk; x += nt)
         for (int g = m.g4_off[x]; g < m.g4_off[x + 1]; ++g) recblk[g] = x % nblk;
     for (int t = tid; t < nblk; t += nt) {
         blkof[m.blk_a[t] * nel + m.blk_b[t]] = t;
         blkof[m.blk_b[t] * nel + m.blk_a[t]] = t;
+    }
+    // Resident mode: one round per request of the mailbox.  Thread 0 polls
+    // (bounded: kResidentPolls reads of host memory, then the kernel exits)
+    // and broadcasts the request through shared memory; -1 ends the loop.
+    ResidentBox* box = a.box;
+    int served = box ? box->ack : 0;
+    int* cmd = status + 1;
+    for (int round = 0;; ++round) {
+        if (box) {
+            if (tid == 0) {
+                // one read of host memory per poll (about a microsecond over
+                // the bus); the quit flag every 16 polls
+                int r = -1;
+                for (int it = 0; it < kResidentPolls; ++it) {
+                    const int q = box->req;
+                    if (q != served) {
+                        r = q;
+                        break;
+                    }
+                    if ((it & 15) == 15 && box->quit) break;
+                }
+                __threadfence_system();  // the request's inputs are read after its number
+                cmd[0] = r;
+            }
+            __syncthreads();
+            const int r = cmd[0];
+            __syncthreads();
+            if (r < 0) break;
+            served = r;
+        } else if (round > 0) {
+            break;
+        }
+    // a request's inputs are read past the caches (the host rewrites them)
+    for (int q = tid; q < n3; q += nt) {
+        pos[q] = a.inline_in ? a.in_pos[q] : box ? ((volatile const double*)a.pos)[q] : a.pos[q];
+        mom[q] = a.eval_only ? 0.0 : a.mom[q];
+        F[q] = a.eval_only ? 0.0 : a.force[q];
+    }
+    for (int i = tid; i < N; i += nt) {
+        mass[i] = a.eval_only ? 1.0 : a.mass[i];
+        elem[i] = a.inline_in ? a.in_elem[i] : box ? ((volatile const int*)a.elem)[i] : a.elem[i];
     }
     if (tid == 0) status[0] = 0;
     __syncthreads();
@@ -808,6 +843,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_tiny_md(DevModel m, TinyArgs a)
             a.acc[1] += a.nsteps;
         }
     }
+    if (box) {
+        // every thread's outputs are visible to the host before the answer
+        __threadfence_system();
+        __syncthreads();
+        if (tid == 0) box->ack = served;
+    }
+    }  // rounds
+    if (box && tid == 0) {
+        __threadfence_system();
+        box->exited = 1;
+    }
 }
 
 // Shared-memory layout of the item-parallel form; SIZE_MAX if it does not fit.
@@ -852,6 +898,26 @@ size_t small_md_smem_bytes(const DevModel& m, int natoms) {
 }
 
 bool small_md_tiny(const DevModel& m, int natoms) { return tiny_md_layout(m, natoms, nullptr) != SIZE_MAX; }
+
+int launch_small_resident(const DevModel& m, int natoms, ResidentBox* box, cudaStream_t s) {
+    TinyArgs ta{};
+    const size_t tsm = tiny_md_layout(m, natoms, &ta);
+    if (tsm == SIZE_MAX) return 0;
+    ta.natoms = natoms;
+    ta.nsteps = 1;
+    ta.dt = 0.0;
+    ta.rc2 = m.max_rc * m.max_rc;
+    ta.pos = box->pos;
+    ta.force = box->force;
+    ta.energy = &box->energy;
+    ta.acc = box->acc;
+    ta.elem = box->elem;
+    ta.eval_only = 1;
+    ta.box = box;
+    cudaFuncSetAttribute(k_tiny_md, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+    k_tiny_md<<<1, kThreads, tsm, s>>>(m, ta);
+    return 1;
+}
 
 int launch_small_md(const Batch& b, const DevModel& m, const SmallMdArgs& x, cudaStream_t s) {
     TinyArgs ta{};

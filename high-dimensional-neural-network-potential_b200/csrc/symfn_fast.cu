@@ -945,7 +945,6 @@ __device__ __forceinline__ void grad_pairs(const FSmem<T>& s, const DevModel& m,
             const T fcp = fj * fk * fjk;
             const T R = a.w * a.w + bq.w * bq.w + rjk2;
             T Y[NE];
-#pragma unroll
             eta_exps<NE, true>(m, ne, R, Y);
             T SA[NE], SC[NE];
 #pragma unroll

@@ -113,7 +113,14 @@ int hdnnp_ctx_set_precision(hdnnp_ctx* c, int precision);
  * thread block that builds the lists by direct search and keeps every
  * intermediate on chip, between one copy in and one copy out; 0 runs it
  * through the general pipeline (same results within rounding; the
- * intermediates of hdnnp_debug_fetch exist only then).                      */
+ * intermediates of hdnnp_debug_fetch exist only then).
+ * "small_resident" (default 1): such molecules that fit the kernel's
+ * item-parallel form are served by a resident copy of it that stays on one
+ * SM between calls and takes each call from a mailbox in mapped host memory
+ * (no launch per call, warm caches; same results).  It leaves by itself
+ * after a few milliseconds without a call, and when the context is freed or
+ * the option is set to 0; while it waits it holds one SM and a
+ * device-wide synchronisation waits for it to leave.                        */
 int hdnnp_ctx_set_option(hdnnp_ctx* c, const char* name, int value);
 
 /* ---------------------------------------------------------------- evaluation
@@ -254,7 +261,8 @@ int hdnnp_dEdLat_to_stress(const double* lat, const double* dEdLat, double* stre
  * entries filled.                                                             */
 int hdnnp_debug_fetch(hdnnp_ctx* c, const char* what, void* host, size_t bytes);
 
-/* Kernel launches issued by the last evaluation on `c`. */
+/* Kernel launches issued by the last evaluation on `c` (0 when the
+ * context's resident single-block kernel served it: option "small_resident"). */
 int hdnnp_last_launch_count(hdnnp_ctx* c, int* launches);
 
 /* The branch-free FP64 functions that the symmetry-function kernels use for
